@@ -1,0 +1,324 @@
+"""ctypes bindings of the test oracles.
+
+TEST INFRASTRUCTURE ONLY: imported by tests/, by __graft_entry__.smoke() and by
+bench.py's CPU-baseline / reference legs, never by the product package.
+
+* ``Bloom`` / ``Cuckoo`` wrap liboracle.so, the C restatement (dtl_oracle.c).
+* ``RefLib`` wraps oracle/_ref/libdtlref_*.so, the reference's own filter logic
+  compiled from its sources (see oracle/Makefile); absent when not built.
+"""
+import ctypes as C
+import os
+
+import numpy as np
+
+HERE = os.path.dirname(os.path.abspath(__file__))
+_u32p = np.ctypeslib.ndpointer(np.uint32, flags="C_CONTIGUOUS")
+
+
+class _Addr(C.Structure):
+    _fields_ = [("mode", C.c_uint32), ("block_cnt", C.c_uint32), ("block_cnt_log2", C.c_uint32),
+                ("block_cnt_mask", C.c_uint32), ("magic", C.c_uint32), ("shift", C.c_uint32)]
+
+
+class _BloomS(C.Structure):
+    _fields_ = [("word_bytes", C.c_uint32), ("w", C.c_uint32), ("s", C.c_uint32), ("z", C.c_uint32),
+                ("k", C.c_uint32), ("addr", _Addr), ("m", C.c_uint64), ("m_actual", C.c_uint64),
+                ("word_cnt", C.c_uint64), ("size_u64", C.c_uint64)]
+
+
+class _CuckooS(C.Structure):
+    _fields_ = [("t", C.c_uint32), ("b", C.c_uint32), ("bytes_per_bucket", C.c_uint32), ("addr", _Addr),
+                ("m", C.c_uint64), ("m_actual", C.c_uint64), ("table_words_u32", C.c_uint64),
+                ("size_u64", C.c_uint64), ("alloc_u64", C.c_uint64)]
+
+
+_lib = None
+
+
+def lib():
+    global _lib
+    if _lib is None:
+        path = os.path.join(HERE, "liboracle.so")
+        if not os.path.exists(path):
+            raise RuntimeError("oracle/liboracle.so is not built (make -C oracle)")
+        L = C.CDLL(path)
+        L.orc_hash.restype = C.c_uint32
+        L.orc_hash.argtypes = [C.c_uint32, C.c_uint32]
+        L.orc_next_cheap_magic.restype = C.c_int
+        L.orc_next_cheap_magic.argtypes = [C.c_uint32] + [C.POINTER(C.c_uint32)] * 3
+        L.orc_fast_mod.restype = C.c_uint32
+        L.orc_fast_mod.argtypes = [C.c_uint32] * 4
+        L.orc_bloom_init.restype = C.c_int
+        L.orc_bloom_init.argtypes = [C.POINTER(_BloomS)] + [C.c_uint32] * 5 + [C.c_uint64]
+        L.orc_bloom_insert.argtypes = [C.POINTER(_BloomS), C.c_void_p, _u32p, C.c_uint64, C.c_int]
+        L.orc_bloom_contains.restype = C.c_int
+        L.orc_bloom_contains.argtypes = [C.POINTER(_BloomS), C.c_void_p, C.c_uint32, C.c_int]
+        L.orc_bloom_batch_contains.restype = C.c_uint64
+        L.orc_bloom_batch_contains.argtypes = [C.POINTER(_BloomS), C.c_void_p, _u32p, C.c_uint32,
+                                               _u32p, C.c_uint32, C.c_int]
+        L.orc_bloom_batch_contains_mt.restype = C.c_uint64
+        L.orc_bloom_batch_contains_mt.argtypes = [C.POINTER(_BloomS), C.c_void_p, _u32p, C.c_uint64,
+                                                  _u32p, C.c_int]
+        L.orc_bloom_bits.argtypes = [C.POINTER(_BloomS), C.c_uint32, C.c_int, _u32p, _u32p]
+        L.orc_cuckoo_init.restype = C.c_int
+        L.orc_cuckoo_init.argtypes = [C.POINTER(_CuckooS), C.c_uint32, C.c_uint32, C.c_uint64]
+        L.orc_cuckoo_insert.restype = C.c_int
+        L.orc_cuckoo_insert.argtypes = [C.POINTER(_CuckooS), C.c_void_p, _u32p, C.c_uint64, C.c_uint64]
+        L.orc_cuckoo_contains.restype = C.c_int
+        L.orc_cuckoo_contains.argtypes = [C.POINTER(_CuckooS), C.c_void_p, C.c_uint32]
+        L.orc_cuckoo_batch_contains.restype = C.c_uint64
+        L.orc_cuckoo_batch_contains.argtypes = [C.POINTER(_CuckooS), C.c_void_p, _u32p, C.c_uint32,
+                                                _u32p, C.c_uint32]
+        L.orc_cuckoo_count_occupied.restype = C.c_uint64
+        L.orc_cuckoo_count_occupied.argtypes = [C.POINTER(_CuckooS), C.c_void_p]
+        L.orc_cuckoo_read_tag.restype = C.c_uint32
+        L.orc_cuckoo_read_tag.argtypes = [C.POINTER(_CuckooS), C.c_void_p, C.c_uint64, C.c_uint32]
+        L.orc_cuckoo_index_tag.argtypes = [C.POINTER(_CuckooS), C.c_uint32] + [C.POINTER(C.c_uint32)] * 3
+        _lib = L
+    return _lib
+
+
+def _keys(keys):
+    return np.ascontiguousarray(keys, dtype=np.uint32)
+
+
+def next_cheap_magic(n):
+    d, mg, sh = C.c_uint32(), C.c_uint32(), C.c_uint32()
+    if not lib().orc_next_cheap_magic(n, C.byref(d), C.byref(mg), C.byref(sh)):
+        raise ValueError("no cheap magic divisor")
+    return d.value, mg.value, sh.value
+
+
+class Bloom:
+    """C restatement of one blocked Bloom filter config (data owned by caller)."""
+
+    def __init__(self, word_bytes, w, s, z, k, m):
+        self.s_ = _BloomS()
+        rc = lib().orc_bloom_init(C.byref(self.s_), word_bytes, w, s, z, k, m)
+        if rc:
+            raise ValueError(f"invalid bloom config rc={rc}")
+
+    @property
+    def size_u64(self):
+        return self.s_.size_u64
+
+    @property
+    def word_cnt(self):
+        return self.s_.word_cnt
+
+    @property
+    def m_actual(self):
+        return self.s_.m_actual
+
+    @property
+    def block_cnt(self):
+        return self.s_.addr.block_cnt
+
+    @property
+    def magic(self):
+        return self.s_.addr.mode == 1
+
+    def alloc(self):
+        return np.zeros(max(1, self.size_u64), dtype=np.uint64)
+
+    def insert(self, data, keys, stale_k8=True):
+        k = _keys(keys)
+        lib().orc_bloom_insert(C.byref(self.s_), data.ctypes.data, k, len(k), int(stale_k8))
+
+    def contains(self, data, key, stale_k8=True):
+        return bool(lib().orc_bloom_contains(C.byref(self.s_), data.ctypes.data, int(key), int(stale_k8)))
+
+    def batch_contains(self, data, keys, match_offset=0, stale_k8=True):
+        k = _keys(keys)
+        out = np.zeros(max(1, len(k)), dtype=np.uint32)
+        n = lib().orc_bloom_batch_contains(C.byref(self.s_), data.ctypes.data, k, len(k), out,
+                                           match_offset & 0xFFFFFFFF, int(stale_k8))
+        return out[:n].copy()
+
+    def batch_contains_mt(self, data, keys, threads):
+        k = _keys(keys)
+        out = np.zeros(max(1, len(k)), dtype=np.uint32)
+        return lib().orc_bloom_batch_contains_mt(C.byref(self.s_), data.ctypes.data, k, len(k), out,
+                                                 threads)
+
+    def bits(self, key, stale_k8=True):
+        wi = np.zeros(16, dtype=np.uint32)
+        bi = np.zeros(16, dtype=np.uint32)
+        lib().orc_bloom_bits(C.byref(self.s_), int(key), int(stale_k8), wi, bi)
+        return wi[: self.s_.k].copy(), bi[: self.s_.k].copy()
+
+
+class Cuckoo:
+    """C restatement of one cuckoo filter config (data owned by caller)."""
+
+    def __init__(self, t, b, m):
+        self.s_ = _CuckooS()
+        rc = lib().orc_cuckoo_init(C.byref(self.s_), t, b, m)
+        if rc:
+            raise ValueError(f"invalid cuckoo config rc={rc}")
+
+    @property
+    def alloc_u64(self):
+        return self.s_.alloc_u64
+
+    @property
+    def size_u64(self):
+        return self.s_.size_u64
+
+    @property
+    def bucket_cnt(self):
+        return self.s_.addr.block_cnt
+
+    @property
+    def table_words_u32(self):
+        return self.s_.table_words_u32
+
+    def alloc(self):
+        return np.zeros(self.alloc_u64, dtype=np.uint64)
+
+    def insert(self, data, keys, seed=1):
+        k = _keys(keys)
+        return bool(lib().orc_cuckoo_insert(C.byref(self.s_), data.ctypes.data, k, len(k), seed))
+
+    def contains(self, data, key):
+        return bool(lib().orc_cuckoo_contains(C.byref(self.s_), data.ctypes.data, int(key)))
+
+    def batch_contains(self, data, keys, match_offset=0):
+        k = _keys(keys)
+        out = np.zeros(max(1, len(k)), dtype=np.uint32)
+        n = lib().orc_cuckoo_batch_contains(C.byref(self.s_), data.ctypes.data, k, len(k), out,
+                                            match_offset & 0xFFFFFFFF)
+        return out[:n].copy()
+
+    def count_occupied(self, data):
+        return lib().orc_cuckoo_count_occupied(C.byref(self.s_), data.ctypes.data)
+
+    def index_tag(self, key):
+        a, b, t = C.c_uint32(), C.c_uint32(), C.c_uint32()
+        lib().orc_cuckoo_index_tag(C.byref(self.s_), int(key), C.byref(a), C.byref(b), C.byref(t))
+        return a.value, b.value, t.value
+
+
+# --------------------------------------------------------------------------
+# The reference compiled from its sources (oracle/_ref)
+# --------------------------------------------------------------------------
+def _cpu_flags():
+    try:
+        with open("/proc/cpuinfo") as f:
+            for line in f:
+                if line.startswith("flags"):
+                    return set(line.split(":", 1)[1].split())
+    except OSError:
+        pass
+    return set()
+
+
+class RefLib:
+    """The reference's filter logic (oracle/_ref/libdtlref_{avx512,avx2}.so)."""
+
+    def __init__(self, variant=None):
+        flags = _cpu_flags()
+        if variant is None:
+            variant = "avx512" if {"avx512f", "avx512bw", "avx512dq", "avx512vl"} <= flags else "avx2"
+        path = os.path.join(HERE, "_ref", f"libdtlref_{variant}.so")
+        if not os.path.exists(path):
+            raise FileNotFoundError(path)
+        self.variant = variant
+        self.path = path
+        L = C.CDLL(path)
+        vp = C.c_void_p
+        L.ref_simd_lanes.restype = C.c_int
+        L.ref_bloom_create.restype = vp
+        L.ref_bloom_create.argtypes = [C.c_uint32] * 5 + [C.c_uint64]
+        L.ref_cuckoo_create.restype = vp
+        L.ref_cuckoo_create.argtypes = [C.c_uint32, C.c_uint32, C.c_uint64]
+        L.ref_instance_count.restype = C.c_int
+        L.ref_instance_count.argtypes = [C.c_int]
+        L.ref_destroy.argtypes = [vp]
+        L.ref_word_cnt.restype = C.c_uint64
+        L.ref_word_cnt.argtypes = [vp]
+        L.ref_length.restype = C.c_uint64
+        L.ref_length.argtypes = [vp]
+        L.ref_insert.restype = C.c_int
+        L.ref_insert.argtypes = [vp, vp, _u32p, C.c_uint32]
+        L.ref_contains.restype = C.c_int
+        L.ref_contains.argtypes = [vp, vp, C.c_uint32]
+        L.ref_batch_contains.restype = C.c_uint64
+        L.ref_batch_contains.argtypes = [vp, vp, _u32p, C.c_uint32, _u32p, C.c_uint32, C.c_int]
+        L.ref_count_occupied.restype = C.c_uint64
+        L.ref_count_occupied.argtypes = [vp, vp]
+        L.ref_batch_contains_mt.restype = C.c_uint64
+        L.ref_batch_contains_mt.argtypes = [vp, vp, _u32p, C.c_uint64, _u32p, C.c_int, C.c_int]
+        L.ref_insert_mt.argtypes = [vp, vp, _u32p, C.c_uint64, C.c_int]
+        L.ref_next_cheap_magic.restype = C.c_int
+        L.ref_next_cheap_magic.argtypes = [C.c_uint32] + [C.POINTER(C.c_uint32)] * 3
+        self.L = L
+        self.lanes = L.ref_simd_lanes()
+
+    def bloom(self, word_bytes, w, s, z, k, m):
+        h = self.L.ref_bloom_create(word_bytes, w, s, z, k, m)
+        return _RefFilter(self, h) if h else None
+
+    def next_cheap_magic(self, n):
+        d, mg, sh = C.c_uint32(), C.c_uint32(), C.c_uint32()
+        if not self.L.ref_next_cheap_magic(n, C.byref(d), C.byref(mg), C.byref(sh)):
+            raise ValueError("no cheap magic divisor")
+        return d.value, mg.value, sh.value
+
+    def cuckoo(self, t, b, m):
+        h = self.L.ref_cuckoo_create(t, b, m)
+        return _RefFilter(self, h) if h else None
+
+
+class _RefFilter:
+    def __init__(self, ref, h):
+        self.ref, self.h = ref, h
+
+    def __del__(self):
+        try:
+            self.ref.L.ref_destroy(self.h)
+        except Exception:
+            pass
+
+    @property
+    def word_cnt(self):
+        return self.ref.L.ref_word_cnt(self.h)
+
+    @property
+    def length(self):
+        return self.ref.L.ref_length(self.h)
+
+    def insert(self, data, keys):
+        k = _keys(keys)
+        return bool(self.ref.L.ref_insert(self.h, data.ctypes.data, k, len(k)))
+
+    def insert_mt(self, data, keys, threads):
+        k = _keys(keys)
+        self.ref.L.ref_insert_mt(self.h, data.ctypes.data, k, len(k), threads)
+
+    def contains(self, data, key):
+        return bool(self.ref.L.ref_contains(self.h, data.ctypes.data, int(key)))
+
+    def batch_contains(self, data, keys, match_offset=0, unroll=1):
+        k = _keys(keys)
+        out = np.zeros(len(k) + 16, dtype=np.uint32)
+        n = self.ref.L.ref_batch_contains(self.h, data.ctypes.data, k, len(k), out,
+                                          match_offset & 0xFFFFFFFF, unroll)
+        return out[:n].copy()
+
+    def batch_contains_mt(self, data, keys, threads, unroll=1, out=None):
+        k = _keys(keys)
+        if out is None:
+            out = np.zeros(len(k) + 16, dtype=np.uint32)
+        return self.ref.L.ref_batch_contains_mt(self.h, data.ctypes.data, k, len(k), out, threads, unroll)
+
+    def count_occupied(self, data):
+        return self.ref.L.ref_count_occupied(self.h, data.ctypes.data)
+
+
+def try_reflib():
+    try:
+        return RefLib()
+    except (FileNotFoundError, OSError):
+        return None
