@@ -1,0 +1,418 @@
+#!/usr/bin/env python3
+"""Probe throughput of the DTL filter path on B200 (and of the reference on the host).
+
+Workload (default, "sectorized_dram"): the cache-sectorized blocked Bloom
+filter of the reference -- 64-byte blocks of 8 x 64-bit words, one sector per
+word, k = 8 (u64, w=8, s=8, k=8) -- at 16 bits per key: build n = 2^28 keys
+(512 MiB of filter words, DRAM-resident), probe 2^28 u32 keys per GPU of which
+10 % are members.  A step is one batch_contains over the 2^28 probe keys,
+writing the ascending match positions.  Inputs (1 GiB keys + 512 MiB filter)
+exceed the 126 MB L2, so no flush is needed between steps.
+
+  python bench.py [--gpus N] [--steps K] [--warmup W] [--impl reference]
+
+Prints one JSON line on rank 0.  Multi-GPU: one process per GPU (torchrun),
+each rank probes its own 2^28-key slice of the probe stream against a
+replicated filter (weak scaling; the only collectives are the barrier and the
+max-over-ranks of the timings).
+"""
+import argparse
+import json
+import os
+import statistics
+import subprocess
+import sys
+import tempfile
+import threading
+import time
+
+ROOT = os.path.dirname(os.path.abspath(__file__))
+sys.path.insert(0, os.path.join(ROOT, "bloomfilter-bsd_b200"))
+
+WORKLOADS = {
+    # name: (word_size, w, s, z, k, log2 n, bits/key, log2 probes, hit ratio)
+    "sectorized_dram": (8, 8, 8, 1, 8, 28, 16, 28, 0.10),
+    "sectorized_l2": (8, 8, 8, 1, 8, 22, 16, 28, 0.10),
+    "register_blocked": (4, 1, 1, 1, 4, 20, 16, 24, 0.10),
+}
+SEED = 20240601
+
+
+def parse():
+    ap = argparse.ArgumentParser()
+    ap.add_argument("--gpus", type=int, default=1)
+    ap.add_argument("--steps", type=int, default=20)
+    ap.add_argument("--warmup", type=int, default=5)
+    ap.add_argument("--impl", choices=("dtlg", "reference"), default="dtlg")
+    ap.add_argument("--workload", choices=sorted(WORKLOADS), default="sectorized_dram")
+    ap.add_argument("--no-cpu-baseline", action="store_true")
+    ap.add_argument("--no-e2e", action="store_true")
+    return ap.parse_args()
+
+
+def workload_config(name, n_gpus):
+    wb, w, s, z, k, ln, bpk, lp, h = WORKLOADS[name]
+    return {
+        "workload": name,
+        "filter": f"blocked Bloom u{wb * 8} w={w} s={s} z={z} k={k}",
+        "bits_per_key": bpk, "build_keys": 1 << ln, "probe_keys_per_gpu": 1 << lp,
+        "global_batch": (1 << lp) * n_gpus, "hit_ratio": h,
+        "filter_bytes": (1 << ln) * bpk // 8, "parallelism": f"dp{n_gpus} (replicated filter, sharded probes)",
+        "l2_flush": "inputs larger than L2 (keys 4 B/key x probes + filter words)",
+    }
+
+
+# ---------------------------------------------------------------------------
+class ClockSampler:
+    """nvidia-smi clocks / throttle reasons sampled during the timed region."""
+
+    Q = ("index,clocks.sm,clocks.max.sm,power.draw,clocks_event_reasons.active,"
+         "clocks_event_reasons.hw_slowdown,clocks_event_reasons.hw_thermal_slowdown,"
+         "clocks_event_reasons.sw_thermal_slowdown,clocks_event_reasons.sw_power_cap")
+
+    def __init__(self, gpu_index):
+        self.gpu = gpu_index
+        self.proc = None
+        self.path = None
+
+    def start(self):
+        try:
+            fd, self.path = tempfile.mkstemp(suffix=".csv")
+            os.close(fd)
+            self.proc = subprocess.Popen(
+                ["nvidia-smi", f"--id={self.gpu}", f"--query-gpu={self.Q}", "--format=csv,noheader,nounits",
+                 "-lms", "100"], stdout=open(self.path, "w"), stderr=subprocess.DEVNULL)
+        except Exception:
+            self.proc = None
+
+    def stop(self):
+        if not self.proc:
+            return None
+        self.proc.terminate()
+        try:
+            self.proc.wait(timeout=5)
+        except Exception:
+            self.proc.kill()
+        sm, mx, reasons = [], None, set()
+        names = ["hw_slowdown", "hw_thermal_slowdown", "sw_thermal_slowdown", "sw_power_cap"]
+        for line in open(self.path):
+            p = [x.strip() for x in line.split(",")]
+            if len(p) < 9:
+                continue
+            try:
+                sm.append(float(p[1]))
+                mx = float(p[2])
+            except ValueError:
+                continue
+            for nm, v in zip(names, p[5:9]):
+                if v.lower() == "active":
+                    reasons.add(nm)
+        os.unlink(self.path)
+        if not sm:
+            return None
+        return {"sm_mhz": statistics.median(sm), "sm_max_mhz": mx, "reasons": sorted(reasons),
+                "samples": len(sm)}
+
+
+def load_traffic_profile():
+    """DRAM bytes per probed key of the probe kernel from the committed ncu summary."""
+    path = os.path.join(ROOT, "profiles", "probe_traffic.json")
+    try:
+        with open(path) as f:
+            return json.load(f)
+    except OSError:
+        return None
+
+
+def load_peaks():
+    try:
+        with open(os.path.join(ROOT, "MEASURED_PEAKS.json")) as f:
+            p = json.load(f)
+        return float(p["hbm_gbs"]), "measured"
+    except Exception:
+        return 6650.0, "fallback"
+
+
+# ---------------------------------------------------------------------------
+def cpu_reference_probe(words_np, cfg, n_build, probe_np, threads, budget_s, want_kind="reference"):
+    """The reference's own SIMD batch_contains (oracle/_ref) -- or, if that
+    library is absent, the C restatement -- on a bounded sample of the probe
+    stream, all host threads.  Returns (keys/s, kind, sample keys, count)."""
+    sys.path.insert(0, os.path.join(ROOT, "oracle"))
+    import numpy as np
+
+    import oracle as O
+    wb, w, s, z, k = cfg
+    m = n_build * 16
+    ref = O.try_reflib() if want_kind == "reference" else None
+    out = np.empty(len(probe_np) + 64, dtype=np.uint32)
+    if ref is not None:
+        f = ref.bloom(wb, w, s, z, k, m)
+        kind = "reference"
+        run = lambda keys: f.batch_contains_mt(words_np, keys, threads, unroll=1, out=out)  # noqa: E731
+    else:
+        f = O.Bloom(wb, w, s, z, k, m)
+        kind = "port"
+        run = lambda keys: f.batch_contains_mt(words_np, keys, threads)  # noqa: E731
+    # size the sample so one pass takes about budget_s
+    n = min(len(probe_np), 1 << 20)
+    t0 = time.perf_counter()
+    run(probe_np[:n])
+    dt = max(time.perf_counter() - t0, 1e-6)
+    n = int(min(len(probe_np), max(n, n * budget_s / dt)))
+    best = None
+    cnt = 0
+    for _ in range(2):
+        t0 = time.perf_counter()
+        cnt = run(probe_np[:n])
+        dt = time.perf_counter() - t0
+        best = dt if best is None else min(best, dt)
+    return n / best, kind, n, cnt, (ref.variant if ref is not None else "c")
+
+
+# ---------------------------------------------------------------------------
+def run_dtlg(args):
+    import numpy as np
+    import torch
+    import torch.distributed as dist
+
+    import dtlg
+    from dtlg import keygen
+
+    rank = int(os.environ.get("RANK", "0"))
+    world = int(os.environ.get("WORLD_SIZE", "1"))
+    local = int(os.environ.get("LOCAL_RANK", "0"))
+    torch.cuda.set_device(local)
+    if world > 1:
+        from datetime import timedelta
+        dist.init_process_group("nccl", timeout=timedelta(seconds=300), device_id=torch.device("cuda", local))
+
+    wb, w, s, z, k, ln, bpk, lp, hit = WORKLOADS[args.workload]
+    n_build, P = 1 << ln, 1 << lp
+    m = n_build * bpk
+    cfg = dtlg.blocked_bloomfilter_config(k=k, word_size=wb, word_cnt_per_block=w, sector_cnt=s, zone_cnt=z)
+    f = dtlg.construct(cfg, m)
+    words = f.alloc_filter_data()
+    bk = keygen.build_keys_torch(n_build, SEED)
+    assert f.batch_insert(words, bk)
+    del bk
+    # this rank's slice of the probe stream; positions are global (offset)
+    start = rank * P
+    keys, member = keygen.probe_keys_torch(n_build, P, hit, SEED, start=start)
+    n_members = int(member.sum().item())
+    del member
+    out = torch.empty(P, dtype=torch.int32, device="cuda")
+    cnt_dev = torch.zeros(1, dtype=torch.int64, device="cuda")
+    ws_bytes = dtlg.lib().dtlg_probe_workspace_size(P)
+    ws = torch.empty(ws_bytes, dtype=torch.uint8, device="cuda")
+    stream = torch.cuda.current_stream()
+    L = dtlg.lib()
+    import ctypes as C
+
+    def step():
+        st = L.dtlg_batch_contains_ws(f._h, C.c_void_p(words.data_ptr()), C.c_void_p(keys.data_ptr()), P,
+                                      C.c_void_p(out.data_ptr()), start & 0xFFFFFFFF, C.c_void_p(cnt_dev.data_ptr()),
+                                      C.c_void_p(ws.data_ptr()), ws_bytes, C.c_void_p(stream.cuda_stream))
+        if st:
+            raise RuntimeError(f"dtlg_batch_contains_ws failed: {st}")
+
+    for _ in range(max(3, args.warmup)):
+        step()
+    torch.cuda.synchronize()
+    count = int(cnt_dev.item())
+    # correctness of the bench's own output: every member found, positions in range
+    assert count >= n_members, (count, n_members)
+    if world > 1:
+        dist.barrier()
+    torch.cuda.synchronize()
+    clocks = ClockSampler(local)
+    clocks.start()
+    evs = [(torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)) for _ in range(args.steps)]
+    t_start = torch.cuda.Event(enable_timing=True)
+    t_end = torch.cuda.Event(enable_timing=True)
+    t_start.record(stream)
+    for i in range(args.steps):
+        evs[i][0].record(stream)
+        step()
+        evs[i][1].record(stream)
+    t_end.record(stream)
+    torch.cuda.synchronize()
+    if world > 1:
+        dist.barrier()
+    clk = clocks.stop()
+    total_ms = t_start.elapsed_time(t_end)
+    per_launch_ms = [a.elapsed_time(b) for a, b in evs]
+    t = torch.tensor([total_ms], dtype=torch.float64, device="cuda")
+    if world > 1:
+        dist.all_reduce(t, op=dist.ReduceOp.MAX)
+    total_ms = float(t.item())
+    ms_per_step = total_ms / args.steps
+    value = world * P / (ms_per_step / 1e3) / 1e9  # Gkeys/s, whole job
+
+    # roofline of the probe kernel (one launch per step)
+    mu = count / P
+    dram_resident = m // 8 > 126 * 2 ** 20
+    S = -(-(w * wb) // 32) if dram_resident else 0
+    alg_bytes_per_key = 4 + 4 * mu + 32 * S
+    launch_ms = statistics.mean(per_launch_ms)
+    achieved = P * alg_bytes_per_key / (launch_ms / 1e3) / 1e9
+    peak, peak_kind = load_peaks()
+    prof = load_traffic_profile()
+    traffic = None
+    if prof and prof.get("workload") == args.workload:
+        traffic = prof["dram_bytes_per_key"] * P
+
+    result = {
+        "metric": "probe Gkeys/s (batch_contains, ascending match positions)",
+        "value": round(value, 3), "unit": "Gkeys/s", "n_gpus": world, "steps": args.steps,
+        "warmup": max(3, args.warmup), "ms_per_step": round(ms_per_step, 4), "higher_is_better": True,
+        "scaling": "weak", "vs_baseline": None, "dtype": "u32",
+        "data": "synthetic: seeded u32 bijection keys (no dataset is published for this path)",
+        "config": workload_config(args.workload, world),
+        "roofline": {"bound": "hbm", "achieved": round(achieved, 1), "peak": peak, "unit": "GB/s",
+                     "frac": round(achieved / peak, 4), "traffic": traffic,
+                     "peak_source": f"MEASURED_PEAKS.json hbm_gbs ({peak_kind})",
+                     "algorithmic_bytes_per_key": round(alg_bytes_per_key, 3),
+                     "dram_resident": dram_resident},
+        "gpu_launches": args.steps,
+        "match_count_per_gpu": count,
+        "clocks": clk,
+    }
+
+    # end to end through the public host-buffer API (pinned keys in, positions out)
+    if not args.no_e2e:
+        keys_h = torch.empty(P, dtype=torch.int32, pin_memory=True)
+        keys_h.copy_(keys)
+        pos_h = torch.empty(P, dtype=torch.int32, pin_memory=True)
+        del out
+        torch.cuda.empty_cache()
+        cnt = C.c_uint64(0)
+
+        def e2e_step():
+            st = L.dtlg_batch_contains_host(f._h, C.c_void_p(words.data_ptr()), C.c_void_p(keys_h.data_ptr()), P,
+                                            C.c_void_p(pos_h.data_ptr()), start & 0xFFFFFFFF, C.byref(cnt),
+                                            C.c_void_p(stream.cuda_stream))
+            if st:
+                raise RuntimeError(f"dtlg_batch_contains_host failed: {st}")
+
+        e2e_step()
+        torch.cuda.synchronize()
+        assert cnt.value == count
+        e_steps = max(3, min(args.steps, 10))
+        if world > 1:
+            dist.barrier()
+        a, b = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
+        a.record(stream)
+        for _ in range(e_steps):
+            e2e_step()
+        b.record(stream)
+        torch.cuda.synchronize()
+        et = torch.tensor([a.elapsed_time(b) / e_steps], dtype=torch.float64, device="cuda")
+        if world > 1:
+            dist.all_reduce(et, op=dist.ReduceOp.MAX)
+        e_ms = float(et.item())
+        chunks = -(-P // (1 << 24))
+        result["e2e"] = {"value": round(world * P / (e_ms / 1e3) / 1e9, 3), "unit": "Gkeys/s",
+                         "ms_per_step": round(e_ms, 3), "h2d_bytes_per_step": P * 4,
+                         "d2h_bytes_per_step": count * 4 + 8 * chunks,
+                         "api": "dtlg_batch_contains_host (pinned host keys -> host positions)"}
+        result["gpu_launches"] += e_steps * chunks
+
+    # the reference's CPU path on this host, bounded sample (rank 0, N=1 only)
+    if rank == 0 and world == 1 and not args.no_cpu_baseline:
+        try:
+            threads = len(os.sched_getaffinity(0))
+            words_np = words.cpu().numpy().view(np.uint64)
+            probe_np = keys.cpu().numpy().view(np.uint32)
+            rate, kind, n, c, variant = cpu_reference_probe(words_np, (wb, w, s, z, k), n_build, probe_np,
+                                                            threads, budget_s=4.0)
+            result["cpu_baseline"] = {"value": round(rate / 1e9, 4), "unit": "Gkeys/s", "cores": threads,
+                                      "kind": kind,
+                                      "sample": f"first {n} probe keys of this workload, best of 2, "
+                                                f"{threads} threads x 1024-key batches, {variant} build",
+                                      "match_count": c}
+        except Exception as e:  # the baseline is reported, never required
+            result["cpu_baseline"] = {"value": None, "error": str(e)[:200]}
+
+    if rank == 0:
+        print(json.dumps(result), flush=True)
+    if world > 1:
+        dist.barrier()
+        dist.destroy_process_group()
+
+
+def run_reference(args):
+    """The reference's own CPU implementation of the path (oracle/_ref: its
+    blocked_bloomfilter_logic compiled from its sources), all host threads,
+    same workload / metric; rank 0 only."""
+    rank = int(os.environ.get("RANK", "0"))
+    world = int(os.environ.get("WORLD_SIZE", "1"))
+    if rank != 0:
+        return
+    import numpy as np
+    sys.path.insert(0, os.path.join(ROOT, "oracle"))
+    import oracle as O
+    from concurrent.futures import ThreadPoolExecutor
+
+    from dtlg import keygen
+    ref = O.try_reflib()
+    if ref is None:
+        print(json.dumps({"impl": "reference", "unavailable": "oracle/_ref (the reference compiled from its "
+                                                               "sources) is not built on this machine"}))
+        return
+    wb, w, s, z, k, ln, bpk, lp, hit = WORKLOADS[args.workload]
+    n_build, P = 1 << ln, 1 << lp
+    m = n_build * bpk
+    threads = len(os.sched_getaffinity(0))
+    f = ref.bloom(wb, w, s, z, k, m)
+    words = np.zeros((f.word_cnt * wb + 7) // 8, dtype=np.uint64)
+    chunk = 1 << 24
+    with ThreadPoolExecutor(max(1, min(threads, 32))) as ex:
+        parts = list(ex.map(lambda b: keygen.build_keys(min(chunk, n_build - b), SEED, start=b),
+                            range(0, n_build, chunk)))
+        bk = np.concatenate(parts)
+        f.insert_mt(words, bk, threads) if z == 1 else f.insert(words, bk)
+        del bk, parts
+        # probe sample: as many keys as take ~2 s per step on this host
+        probe = np.concatenate(list(ex.map(
+            lambda b: keygen.probe_keys(n_build, min(chunk, P - b), hit, SEED, start=b)[0],
+            range(0, min(P, 1 << 26), chunk))))
+    out = np.empty(len(probe) + 64, dtype=np.uint32)
+    t0 = time.perf_counter()
+    f.batch_contains_mt(words, probe[:1 << 22], threads, unroll=1, out=out)
+    rate0 = (1 << 22) / max(1e-6, time.perf_counter() - t0)
+    n = int(min(len(probe), max(1 << 22, rate0 * 2.0)))
+    for _ in range(max(1, args.warmup)):
+        f.batch_contains_mt(words, probe[:n], threads, unroll=1, out=out)
+    times = []
+    cnt = 0
+    for _ in range(args.steps):
+        t0 = time.perf_counter()
+        cnt = f.batch_contains_mt(words, probe[:n], threads, unroll=1, out=out)
+        times.append(time.perf_counter() - t0)
+    ms = 1e3 * statistics.mean(times)
+    value = n / (ms / 1e3) / 1e9
+    print(json.dumps({
+        "impl": "reference", "metric": "probe Gkeys/s (batch_contains, ascending match positions)",
+        "value": round(value, 4), "unit": "Gkeys/s", "n_gpus": world, "steps": args.steps,
+        "warmup": args.warmup, "ms_per_step": round(ms, 3), "higher_is_better": True, "scaling": "weak",
+        "vs_baseline": None, "dtype": "u32", "data": "synthetic: seeded u32 bijection keys",
+        "config": workload_config(args.workload, world),
+        "cpu_baseline": {"value": round(value, 4), "unit": "Gkeys/s", "cores": threads, "kind": "reference",
+                         "sample": f"{n} of the workload's probe keys per step, {threads} threads x 1024-key "
+                                   f"batches (model/benchmark.cpp:123-165), SIMD batch_contains "
+                                   f"({ref.variant}, {ref.lanes} lanes)", "match_count": int(cnt)},
+        "e2e": {"value": round(value, 4), "unit": "Gkeys/s", "h2d_bytes_per_step": 0, "d2h_bytes_per_step": 0},
+    }), flush=True)
+
+
+def main():
+    args = parse()
+    if args.impl == "reference":
+        run_reference(args)
+    else:
+        run_dtlg(args)
+
+
+if __name__ == "__main__":
+    main()

@@ -1,0 +1,412 @@
+// api.cu -- the C ABI of libdtlg.so (include/dtlg.h).
+#include <cuda_runtime.h>
+
+#include <algorithm>
+#include <atomic>
+#include <cstring>
+#include <mutex>
+#include <string>
+#include <vector>
+
+#include "../../include/dtlg.h"
+#include "host_config.hpp"
+#include "registry.hpp"
+
+using namespace dtlg;
+
+struct dtlg_filter {
+  FilterDesc d;
+  const BloomKernels* bk = nullptr;
+  const CuckooKernels* ck = nullptr;
+};
+
+namespace dtlg {
+
+// ---- registry ----------------------------------------------------------------
+static std::vector<BloomKernels>& bloom_table() {
+  static std::vector<BloomKernels> t;
+  return t;
+}
+static std::vector<CuckooKernels>& cuckoo_table() {
+  static std::vector<CuckooKernels> t;
+  return t;
+}
+void register_bloom(const BloomKernels& k) { bloom_table().push_back(k); }
+void register_cuckoo(const CuckooKernels& k) { cuckoo_table().push_back(k); }
+const BloomKernels* find_bloom(uint32_t wb, uint32_t w, uint32_t s, uint32_t z, uint32_t k) {
+  for (const auto& e : bloom_table())
+    if (e.word_bytes == wb && e.w == w && e.s == s && e.z == z && e.k == k) return &e;
+  return nullptr;
+}
+const CuckooKernels* find_cuckoo(uint32_t t, uint32_t b) {
+  for (const auto& e : cuckoo_table())
+    if (e.t == t && e.b == b) return &e;
+  return nullptr;
+}
+int registered_bloom_count() { return static_cast<int>(bloom_table().size()); }
+
+// ---- per-device state ----------------------------------------------------------
+namespace {
+thread_local std::string g_last_cuda_error;
+
+struct DeviceState {
+  bool init = false;
+  int sms = 0;
+  cudaMemPool_t pool = nullptr;
+};
+std::mutex g_mu;
+DeviceState g_dev[64];
+
+dtlg_status cuda_fail(cudaError_t e) {
+  g_last_cuda_error = cudaGetErrorString(e);
+  return DTLG_ERR_CUDA;
+}
+
+#define DTLG_CUDA(x)                         \
+  do {                                       \
+    cudaError_t _e = (x);                    \
+    if (_e != cudaSuccess) return cuda_fail(_e); \
+  } while (0)
+
+dtlg_status device_state(DeviceState** out) {
+  int dev = 0;
+  DTLG_CUDA(cudaGetDevice(&dev));
+  if (dev < 0 || dev >= 64) return DTLG_ERR_CUDA;
+  std::lock_guard<std::mutex> lk(g_mu);
+  DeviceState& s = g_dev[dev];
+  if (!s.init) {
+    DTLG_CUDA(cudaDeviceGetAttribute(&s.sms, cudaDevAttrMultiProcessorCount, dev));
+    // A library-private stream-ordered pool for per-call workspaces; it keeps
+    // its memory between calls instead of returning it at every sync.
+    cudaMemPoolProps props{};
+    props.allocType = cudaMemAllocationTypePinned;
+    props.handleTypes = cudaMemHandleTypeNone;
+    props.location.type = cudaMemLocationTypeDevice;
+    props.location.id = dev;
+    DTLG_CUDA(cudaMemPoolCreate(&s.pool, &props));
+    uint64_t thr = ~0ull;
+    DTLG_CUDA(cudaMemPoolSetAttribute(s.pool, cudaMemPoolAttrReleaseThreshold, &thr));
+    s.init = true;
+  }
+  *out = &s;
+  return DTLG_OK;
+}
+
+// Workspace of one probe call: header (tile counter, error word, count) then
+// one look-back status word per tile.
+struct WsHeader {
+  unsigned int tile_ctr;
+  unsigned int err;
+  unsigned long long count;
+  unsigned long long pad[14];
+};
+static_assert(sizeof(WsHeader) == 128, "header is one 128-byte line");
+
+uint32_t probe_tiles(uint64_t n_phys) { return static_cast<uint32_t>((n_phys + kProbeTile - 1) / kProbeTile); }
+
+dtlg_status check_filter_ptr(const void* p) {
+  if (!p) return DTLG_ERR_NULL;
+  if (reinterpret_cast<uintptr_t>(p) & 15u) return DTLG_ERR_ALIGNMENT;
+  return DTLG_OK;
+}
+
+// Enqueues the probe of `keys[0..n)`; the count goes to count_dev.
+dtlg_status launch_probe(const dtlg_filter* f, const uint64_t* words, const uint32_t* keys, uint32_t n,
+                         uint32_t* out, uint32_t offset, unsigned long long* count_dev, void* ws,
+                         size_t ws_bytes, cudaStream_t stream) {
+  DeviceState* ds = nullptr;
+  dtlg_status st = device_state(&ds);
+  if (st) return st;
+  if (n == 0) {
+    DTLG_CUDA(cudaMemsetAsync(count_dev, 0, sizeof(unsigned long long), stream));
+    return DTLG_OK;
+  }
+  const uint32_t pre = static_cast<uint32_t>((reinterpret_cast<uintptr_t>(keys) & 15u) >> 2);
+  const uint64_t n_phys = static_cast<uint64_t>(n) + pre;
+  const uint32_t tiles = probe_tiles(n_phys);
+  const size_t need = sizeof(WsHeader) + static_cast<size_t>(tiles) * 8;
+  if (ws_bytes < need) return DTLG_ERR_WORKSPACE;
+  DTLG_CUDA(cudaMemsetAsync(ws, 0, need, stream));
+  WsHeader* h = static_cast<WsHeader*>(ws);
+  ProbeArgs a{};
+  a.filter = words;
+  a.keys_al = keys - pre;
+  a.n_phys = n_phys;
+  a.pre = pre;
+  a.match_offset = offset;
+  a.out = out;
+  a.count_out = count_dev;
+  a.status = reinterpret_cast<unsigned long long*>(h + 1);
+  a.tile_ctr = &h->tile_ctr;
+  a.err = &h->err;
+  a.n_tiles = tiles;
+  a.addr = f->d.addr;
+  a.victim_word = f->d.victim_word;
+  const probe_fn fn = f->bk ? f->bk->probe : f->ck->probe;
+  const occ_fn occ = f->bk ? f->bk->probe_blocks_per_sm : f->ck->probe_blocks_per_sm;
+  const int per_sm = std::max(1, occ());
+  const int grid = static_cast<int>(std::min<uint64_t>(tiles, static_cast<uint64_t>(ds->sms) * per_sm));
+  DTLG_CUDA(fn(a, grid, stream));
+  return DTLG_OK;
+}
+
+int grid_for(uint64_t items, int sms) {
+  return static_cast<int>(std::max<uint64_t>(1, std::min<uint64_t>((items + 255) / 256, static_cast<uint64_t>(sms) * 8)));
+}
+
+dtlg_status cuckoo_insert(const dtlg_filter* f, uint64_t* words, const uint32_t* keys, uint32_t n,
+                          uint64_t* failed_out, cudaStream_t stream) {
+  DeviceState* ds = nullptr;
+  dtlg_status st = device_state(&ds);
+  if (st) return st;
+  if (failed_out) *failed_out = 0;
+  if (n == 0) return DTLG_OK;
+  const FilterDesc& d = f->d;
+  const uint64_t slots_n = (static_cast<uint64_t>(d.addr.block_cnt) + 1) * d.b;
+  uint32_t* slots = nullptr;
+  unsigned long long* failed = nullptr;
+  const uint64_t slot_bytes = (slots_n * 4 + 255) & ~255ull;
+  DTLG_CUDA(cudaMallocFromPoolAsync(reinterpret_cast<void**>(&slots), slot_bytes + 256, ds->pool, stream));
+  failed = reinterpret_cast<unsigned long long*>(reinterpret_cast<char*>(slots) + slot_bytes);
+  DTLG_CUDA(cudaMemsetAsync(failed, 0, 8, stream));
+  DTLG_CUDA(cudaMemsetAsync(slots + static_cast<uint64_t>(d.addr.block_cnt) * d.b, 0, d.b * 4, stream));
+  uint32_t* table = reinterpret_cast<uint32_t*>(words);
+  f->ck->unpack(table, slots, d.addr.block_cnt, grid_for(slots_n, ds->sms), stream);
+  const uint32_t pre = static_cast<uint32_t>((reinterpret_cast<uintptr_t>(keys) & 15u) >> 2);
+  CuckooBuildArgs a{};
+  a.table = table;
+  a.slots = slots;
+  a.keys_al = keys - pre;
+  a.n_phys = static_cast<uint64_t>(n) + pre;
+  a.pre = pre;
+  a.table_words = d.word_cnt;
+  a.victim_word = d.victim_word;
+  a.addr = d.addr;
+  a.failed = failed;
+  static std::atomic<uint64_t> seed_ctr{0x243F6A8885A308D3ull};
+  a.seed = seed_ctr.fetch_add(0x9E3779B97F4A7C15ull);
+  f->ck->insert(a, grid_for(a.n_phys, ds->sms), stream);
+  f->ck->pack(table, slots, d.addr.block_cnt, d.word_cnt, grid_for(d.word_cnt, ds->sms), stream);
+  unsigned long long lost = 0;
+  DTLG_CUDA(cudaMemcpyAsync(&lost, failed, 8, cudaMemcpyDeviceToHost, stream));
+  DTLG_CUDA(cudaFreeAsync(slots, stream));
+  DTLG_CUDA(cudaStreamSynchronize(stream));
+  DTLG_CUDA(cudaGetLastError());
+  if (failed_out) *failed_out = lost;
+  return lost ? DTLG_ERR_CUCKOO_FULL : DTLG_OK;
+}
+
+}  // namespace
+}  // namespace dtlg
+
+// =============================================================================
+extern "C" {
+
+const char* dtlg_version(void) { return "dtlg 0.1 (sm_100a)"; }
+
+const char* dtlg_last_cuda_error(void) { return dtlg::g_last_cuda_error.c_str(); }
+
+const char* dtlg_status_string(dtlg_status s) {
+  switch (s) {
+    case DTLG_OK: return "ok";
+    case DTLG_ERR_INVALID_CONFIG: return "invalid configuration";
+    case DTLG_ERR_SIZE: return "filter size out of range (block count must not exceed 2^31)";
+    case DTLG_ERR_NULL: return "null pointer";
+    case DTLG_ERR_ALIGNMENT: return "filter words must be 16-byte aligned";
+    case DTLG_ERR_CUDA: return "CUDA error";
+    case DTLG_ERR_ALLOC: return "allocation failed";
+    case DTLG_ERR_CUCKOO_FULL: return "cuckoo filter full: some keys could not be inserted";
+    case DTLG_ERR_TIMEOUT: return "a bounded device wait timed out";
+    case DTLG_ERR_WORKSPACE: return "workspace too small";
+    case DTLG_ERR_UNSUPPORTED: return "unsupported operation";
+  }
+  return "unknown status";
+}
+
+dtlg_status dtlg_bloom_create(const dtlg_bloom_config* cfg, uint64_t m, dtlg_filter** out) {
+  if (!cfg || !out) return DTLG_ERR_NULL;
+  *out = nullptr;
+  dtlg_filter* f = new dtlg_filter();
+  const int rc = describe_bloom(cfg->word_size, cfg->word_cnt_per_block, cfg->sector_cnt, cfg->zone_cnt,
+                                cfg->k, m, &f->d);
+  if (rc) {
+    delete f;
+    return rc == 1 ? DTLG_ERR_INVALID_CONFIG : DTLG_ERR_SIZE;
+  }
+  f->bk = find_bloom(f->d.word_bytes, f->d.w, f->d.s, f->d.z, f->d.k);
+  if (!f->bk) {
+    delete f;
+    return DTLG_ERR_INVALID_CONFIG;
+  }
+  *out = f;
+  return DTLG_OK;
+}
+
+dtlg_status dtlg_cuckoo_create(const dtlg_cuckoo_config* cfg, uint64_t m, dtlg_filter** out) {
+  if (!cfg || !out) return DTLG_ERR_NULL;
+  *out = nullptr;
+  dtlg_filter* f = new dtlg_filter();
+  const int rc = describe_cuckoo(cfg->bits_per_tag, cfg->tags_per_bucket, m, &f->d);
+  if (rc) {
+    delete f;
+    return rc == 1 ? DTLG_ERR_INVALID_CONFIG : DTLG_ERR_SIZE;
+  }
+  f->ck = find_cuckoo(f->d.t, f->d.b);
+  if (!f->ck) {
+    delete f;
+    return DTLG_ERR_INVALID_CONFIG;
+  }
+  *out = f;
+  return DTLG_OK;
+}
+
+void dtlg_destroy(dtlg_filter* f) { delete f; }
+
+uint64_t dtlg_size_in_bytes(const dtlg_filter* f) { return f ? (f->d.m_actual + 7) / 8 : 0; }
+uint64_t dtlg_size(const dtlg_filter* f) { return f ? f->d.size_u64 : 0; }
+uint64_t dtlg_alloc_words_u64(const dtlg_filter* f) { return f ? f->d.alloc_u64 : 0; }
+int dtlg_kind(const dtlg_filter* f) { return f ? static_cast<int>(f->d.kind) : -1; }
+uint64_t dtlg_block_cnt(const dtlg_filter* f) { return f ? f->d.addr.block_cnt : 0; }
+int dtlg_is_magic(const dtlg_filter* f) { return f ? static_cast<int>(f->d.addr.magic_mode) : 0; }
+
+size_t dtlg_name(const dtlg_filter* f, char* buf, size_t cap) {
+  if (!f) return 0;
+  const std::string s = filter_name(f->d);
+  if (buf && cap > s.size()) {
+    std::memcpy(buf, s.c_str(), s.size() + 1);
+  } else if (buf && cap) {
+    buf[0] = 0;
+  }
+  return s.size();
+}
+
+dtlg_status dtlg_batch_insert(const dtlg_filter* f, uint64_t* words, const uint32_t* keys, uint32_t n,
+                              uint64_t* failed_out, dtlg_stream_t stream_) {
+  cudaStream_t stream = reinterpret_cast<cudaStream_t>(stream_);
+  if (!f) return DTLG_ERR_NULL;
+  if (failed_out) *failed_out = 0;
+  if (n && !keys) return DTLG_ERR_NULL;
+  if (dtlg_status st = check_filter_ptr(words)) return st;
+  if (f->ck) return cuckoo_insert(f, words, keys, n, failed_out, stream);
+  if (n == 0) return DTLG_OK;
+  DeviceState* ds = nullptr;
+  if (dtlg_status st = device_state(&ds)) return st;
+  const uint32_t pre = static_cast<uint32_t>((reinterpret_cast<uintptr_t>(keys) & 15u) >> 2);
+  BuildArgs a{};
+  a.filter = words;
+  a.keys_al = keys - pre;
+  a.n_phys = static_cast<uint64_t>(n) + pre;
+  a.pre = pre;
+  a.addr = f->d.addr;
+  DTLG_CUDA(f->bk->build(a, grid_for((a.n_phys + 3) / 4, ds->sms), stream));
+  return DTLG_OK;
+}
+
+size_t dtlg_probe_workspace_size(uint32_t key_cnt) {
+  return sizeof(WsHeader) + static_cast<size_t>(probe_tiles(static_cast<uint64_t>(key_cnt) + 3)) * 8;
+}
+
+dtlg_status dtlg_batch_contains_ws(const dtlg_filter* f, const uint64_t* words, const uint32_t* keys,
+                                   uint32_t n, uint32_t* out, uint32_t offset, uint64_t* count_dev,
+                                   void* ws, size_t ws_bytes, dtlg_stream_t stream) {
+  if (!f || !count_dev || (n && (!keys || !out)) || !ws) return DTLG_ERR_NULL;
+  if (dtlg_status st = check_filter_ptr(words)) return st;
+  return launch_probe(f, words, keys, n, out, offset, reinterpret_cast<unsigned long long*>(count_dev), ws,
+                      ws_bytes, reinterpret_cast<cudaStream_t>(stream));
+}
+
+dtlg_status dtlg_batch_contains_async(const dtlg_filter* f, const uint64_t* words, const uint32_t* keys,
+                                      uint32_t n, uint32_t* out, uint32_t offset, uint64_t* count_dev,
+                                      dtlg_stream_t stream_) {
+  cudaStream_t stream = reinterpret_cast<cudaStream_t>(stream_);
+  if (!f || !count_dev || (n && (!keys || !out))) return DTLG_ERR_NULL;
+  if (dtlg_status st = check_filter_ptr(words)) return st;
+  DeviceState* ds = nullptr;
+  if (dtlg_status st = device_state(&ds)) return st;
+  const size_t ws_bytes = dtlg_probe_workspace_size(n);
+  void* ws = nullptr;
+  DTLG_CUDA(cudaMallocFromPoolAsync(&ws, ws_bytes, ds->pool, stream));
+  dtlg_status st = launch_probe(f, words, keys, n, out, offset, reinterpret_cast<unsigned long long*>(count_dev),
+                                ws, ws_bytes, stream);
+  cudaFreeAsync(ws, stream);
+  return st;
+}
+
+dtlg_status dtlg_batch_contains(const dtlg_filter* f, const uint64_t* words, const uint32_t* keys, uint32_t n,
+                                uint32_t* out, uint32_t offset, uint64_t* match_cnt, dtlg_stream_t stream_) {
+  cudaStream_t stream = reinterpret_cast<cudaStream_t>(stream_);
+  if (!f || !match_cnt || (n && (!keys || !out))) return DTLG_ERR_NULL;
+  if (dtlg_status st = check_filter_ptr(words)) return st;
+  DeviceState* ds = nullptr;
+  if (dtlg_status st = device_state(&ds)) return st;
+  const size_t ws_bytes = dtlg_probe_workspace_size(n);
+  void* ws = nullptr;
+  DTLG_CUDA(cudaMallocFromPoolAsync(&ws, ws_bytes, ds->pool, stream));
+  WsHeader* h = static_cast<WsHeader*>(ws);
+  dtlg_status st = launch_probe(f, words, keys, n, out, offset, &h->count, ws, ws_bytes, stream);
+  WsHeader host{};
+  if (st == DTLG_OK) {
+    cudaError_t e = cudaMemcpyAsync(&host, h, 16, cudaMemcpyDeviceToHost, stream);
+    if (e != cudaSuccess) st = cuda_fail(e);
+  }
+  cudaFreeAsync(ws, stream);
+  if (st != DTLG_OK) return st;
+  DTLG_CUDA(cudaStreamSynchronize(stream));
+  if (n == 0) host.count = 0;
+  *match_cnt = host.count;
+  return host.err ? DTLG_ERR_TIMEOUT : DTLG_OK;
+}
+
+dtlg_status dtlg_insert(const dtlg_filter* f, uint64_t* words, uint32_t key, dtlg_stream_t stream_) {
+  cudaStream_t stream = reinterpret_cast<cudaStream_t>(stream_);
+  DeviceState* ds = nullptr;
+  if (dtlg_status st = device_state(&ds)) return st;
+  uint32_t* k = nullptr;
+  DTLG_CUDA(cudaMallocFromPoolAsync(reinterpret_cast<void**>(&k), 16, ds->pool, stream));
+  DTLG_CUDA(cudaMemcpyAsync(k, &key, 4, cudaMemcpyHostToDevice, stream));
+  dtlg_status st = dtlg_batch_insert(f, words, k, 1, nullptr, stream_);
+  cudaFreeAsync(k, stream);
+  DTLG_CUDA(cudaStreamSynchronize(stream));
+  return st;
+}
+
+dtlg_status dtlg_contains(const dtlg_filter* f, const uint64_t* words, uint32_t key, int* result,
+                          dtlg_stream_t stream_) {
+  cudaStream_t stream = reinterpret_cast<cudaStream_t>(stream_);
+  if (!result) return DTLG_ERR_NULL;
+  DeviceState* ds = nullptr;
+  if (dtlg_status st = device_state(&ds)) return st;
+  uint32_t* k = nullptr;
+  DTLG_CUDA(cudaMallocFromPoolAsync(reinterpret_cast<void**>(&k), 64, ds->pool, stream));
+  DTLG_CUDA(cudaMemcpyAsync(k, &key, 4, cudaMemcpyHostToDevice, stream));
+  uint64_t cnt = 0;
+  dtlg_status st = dtlg_batch_contains(f, words, k, 1, k + 4, 0, &cnt, stream_);
+  cudaFreeAsync(k, stream);
+  DTLG_CUDA(cudaStreamSynchronize(stream));
+  *result = cnt ? 1 : 0;
+  return st;
+}
+
+dtlg_status dtlg_count_occupied_slots(const dtlg_filter* f, const uint64_t* words, uint64_t* count,
+                                      dtlg_stream_t stream_) {
+  cudaStream_t stream = reinterpret_cast<cudaStream_t>(stream_);
+  if (!f || !count) return DTLG_ERR_NULL;
+  if (!f->ck) return DTLG_ERR_UNSUPPORTED;
+  if (dtlg_status st = check_filter_ptr(words)) return st;
+  DeviceState* ds = nullptr;
+  if (dtlg_status st = device_state(&ds)) return st;
+  unsigned long long* c = nullptr;
+  DTLG_CUDA(cudaMallocFromPoolAsync(reinterpret_cast<void**>(&c), 8, ds->pool, stream));
+  DTLG_CUDA(cudaMemsetAsync(c, 0, 8, stream));
+  const uint64_t slots = static_cast<uint64_t>(f->d.addr.block_cnt) * f->d.b;
+  f->ck->count(reinterpret_cast<const uint32_t*>(words), f->d.addr.block_cnt, f->d.victim_word, c,
+               grid_for(slots, ds->sms), stream);
+  unsigned long long h = 0;
+  DTLG_CUDA(cudaMemcpyAsync(&h, c, 8, cudaMemcpyDeviceToHost, stream));
+  cudaFreeAsync(c, stream);
+  DTLG_CUDA(cudaStreamSynchronize(stream));
+  *count = h;
+  return DTLG_OK;
+}
+
+}  // extern "C"

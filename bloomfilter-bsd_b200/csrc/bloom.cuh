@@ -1,0 +1,158 @@
+// bloom.cuh -- blocked Bloom filter probe / build for one compile-time config.
+//
+// Reference: blocked_bloomfilter_logic.hpp:95-136 (h0 = hash_0(key) selects
+// the block; the block type sets / tests k bits) with the block types of
+// blocked_bloomfilter_block_logic_{sgew,sltw,zoned}.hpp.  The bit layout comes
+// from make_schedule() (common.cuh) and is identical to the reference's scalar
+// insert / contains, so filters built here are byte-identical to CPU builds.
+#pragma once
+
+#include <cstdint>
+
+#include "common.cuh"
+#include "probe.cuh"
+
+namespace dtlg {
+
+template <typename Word, int W, int S, int Z, int K>
+struct BloomCfg {
+  using word_t = Word;
+  static constexpr int kW = W, kS = S, kZ = Z, kK = K;
+  static constexpr int kBlockBytes = W * static_cast<int>(sizeof(Word));
+  static constexpr Schedule sched =
+      make_schedule(static_cast<uint32_t>(sizeof(Word) * 8), W, S, Z, K, /*stale_k8=*/true);
+  static_assert(sched.ok, "config needs a hash function beyond the family");
+};
+
+struct BuildArgs {
+  void* filter;
+  const uint32_t* keys_al;
+  uint64_t n_phys;
+  uint32_t pre;
+  Addr addr;
+};
+
+#ifdef __CUDACC__
+
+template <typename Word>
+__device__ __forceinline__ void atomic_or_word(Word* p, Word m) {
+  if constexpr (sizeof(Word) == 8) {
+    atomicOr(reinterpret_cast<unsigned long long*>(p), static_cast<unsigned long long>(m));
+  } else {
+    atomicOr(reinterpret_cast<unsigned int*>(p), static_cast<unsigned int>(m));
+  }
+}
+
+// Loads a whole block of W words with the widest aligned vector loads.
+template <typename Word, int W>
+__device__ __forceinline__ void load_block(const Word* base, Word (&v)[W]) {
+  constexpr int kBytes = W * static_cast<int>(sizeof(Word));
+  if constexpr (kBytes >= 16) {
+    const uint4* p = reinterpret_cast<const uint4*>(base);
+#pragma unroll
+    for (int i = 0; i < kBytes / 16; i++) {
+      const uint4 x = __ldg(p + i);
+      uint32_t* d = reinterpret_cast<uint32_t*>(&v[0]) + 4 * i;
+      d[0] = x.x; d[1] = x.y; d[2] = x.z; d[3] = x.w;
+    }
+  } else if constexpr (kBytes == 8) {
+    const unsigned long long x = __ldg(reinterpret_cast<const unsigned long long*>(base));
+    *reinterpret_cast<unsigned long long*>(&v[0]) = x;
+  } else {
+    v[0] = static_cast<Word>(__ldg(reinterpret_cast<const unsigned int*>(base)));
+  }
+}
+
+template <class Cfg>
+struct BloomOps {
+  using Word = typename Cfg::word_t;
+  static constexpr Schedule kS = Cfg::sched;
+  static constexpr int kW = Cfg::kW;
+
+  template <int G>
+  __device__ __forceinline__ static Word group_mask(uint32_t key) {
+    constexpr Group g = kS.g[G];
+    Word m = 0;
+    static_for<g.nbit>([&](auto J) {
+      constexpr BitDraw b = g.bit[decltype(J)::value];
+      const uint32_t v = (hash_sel<b.sel>(key) >> b.shift) & ((1u << b.bits) - 1u);
+      m |= Word(1) << (v + b.off);
+    });
+    return m;
+  }
+
+  template <int G>
+  __device__ __forceinline__ static uint32_t group_word(uint32_t key) {
+    constexpr Group g = kS.g[G];
+    if constexpr (g.wbits == 0) {
+      return g.wconst;
+    } else {
+      return g.wconst + ((hash_sel<g.wsel>(key) >> g.wshift) & ((1u << g.wbits) - 1u));
+    }
+  }
+
+  __device__ __forceinline__ static const Word* block_ptr(const void* filter, uint32_t key, const Addr& a) {
+    const uint32_t blk = block_index(key * mul_const(0), a);
+    return static_cast<const Word*>(filter) + static_cast<uint64_t>(blk) * kW;
+  }
+
+  // Every bit of the key set?  ((word & mask) == mask over all touched words,
+  // without early out, as blocked_bloomfilter.hpp:34 configures.)
+  __device__ __forceinline__ static bool contains(const ProbeArgs& a, uint32_t key) {
+    const Word* base = block_ptr(a.filter, key, a.addr);
+    bool ok = true;
+    if constexpr (kS.fixed_words) {
+      Word v[kW];
+      load_block<Word, kW>(base, v);
+      static_for<kS.ng>([&](auto G) {
+        constexpr int g = decltype(G)::value;
+        const Word m = group_mask<g>(key);
+        ok &= (v[kS.g[g].wconst] & m) == m;
+      });
+    } else {
+      static_for<kS.ng>([&](auto G) {
+        constexpr int g = decltype(G)::value;
+        const Word m = group_mask<g>(key);
+        Word x;
+        if constexpr (sizeof(Word) == 8) {
+          x = __ldg(reinterpret_cast<const unsigned long long*>(base) + group_word<g>(key));
+        } else {
+          x = __ldg(reinterpret_cast<const unsigned int*>(base) + group_word<g>(key));
+        }
+        ok &= (x & m) == m;
+      });
+    }
+    return ok;
+  }
+
+  __device__ __forceinline__ static void insert(void* filter, uint32_t key, const Addr& a) {
+    Word* base = const_cast<Word*>(block_ptr(filter, key, a));
+    static_for<kS.ng>([&](auto G) {
+      constexpr int g = decltype(G)::value;
+      atomic_or_word<Word>(base + group_word<g>(key), group_mask<g>(key));
+    });
+  }
+};
+
+// batch_insert (blocked_bloomfilter_logic.hpp:111-117).  The reference inserts
+// sequentially with a CAS-OR per word (..._sgew.hpp:300-325); OR commutes, so
+// concurrent atomic ORs give the same words in any order.
+template <class Cfg>
+__global__ void __launch_bounds__(256) bloom_build_kernel(const __grid_constant__ BuildArgs a) {
+  const uint4* keys4 = reinterpret_cast<const uint4*>(a.keys_al);
+  const uint64_t nvec = (a.n_phys + 3) >> 2;
+  for (uint64_t v = blockIdx.x * static_cast<uint64_t>(blockDim.x) + threadIdx.x; v < nvec;
+       v += static_cast<uint64_t>(gridDim.x) * blockDim.x) {
+    const uint4 kv = __ldcs(keys4 + v);
+    const uint32_t k[4] = {kv.x, kv.y, kv.z, kv.w};
+#pragma unroll
+    for (int q = 0; q < 4; q++) {
+      const uint64_t p = v * 4 + q;
+      if (p >= a.pre && p < a.n_phys) BloomOps<Cfg>::insert(a.filter, k[q], a.addr);
+    }
+  }
+}
+
+#endif  // __CUDACC__
+
+}  // namespace dtlg

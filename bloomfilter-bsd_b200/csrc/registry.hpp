@@ -1,0 +1,108 @@
+// registry.hpp -- table of compiled kernel instantiations, keyed by config.
+#pragma once
+
+#include <cuda_runtime.h>
+
+#include <cstdint>
+
+#include "bloom.cuh"
+#include "cuckoo.cuh"
+#include "probe.cuh"
+
+namespace dtlg {
+
+using probe_fn = cudaError_t (*)(const ProbeArgs&, int grid, cudaStream_t);
+using build_fn = cudaError_t (*)(const BuildArgs&, int grid, cudaStream_t);
+using occ_fn = int (*)();
+
+struct BloomKernels {
+  uint32_t word_bytes, w, s, z, k;
+  probe_fn probe;
+  build_fn build;
+  occ_fn probe_blocks_per_sm;
+};
+
+struct CuckooKernels {
+  uint32_t t, b;
+  probe_fn probe;
+  occ_fn probe_blocks_per_sm;
+  void (*unpack)(const uint32_t* table, uint32_t* slots, uint32_t buckets, int grid, cudaStream_t);
+  void (*insert)(const CuckooBuildArgs&, int grid, cudaStream_t);
+  void (*pack)(uint32_t* table, const uint32_t* slots, uint32_t buckets, uint64_t words, int grid,
+               cudaStream_t);
+  void (*count)(const uint32_t* table, uint32_t buckets, uint64_t victim_word, unsigned long long* out,
+                int grid, cudaStream_t);
+};
+
+void register_bloom(const BloomKernels& k);
+void register_cuckoo(const CuckooKernels& k);
+const BloomKernels* find_bloom(uint32_t word_bytes, uint32_t w, uint32_t s, uint32_t z, uint32_t k);
+const CuckooKernels* find_cuckoo(uint32_t t, uint32_t b);
+int registered_bloom_count();
+
+// Keys per probe tile: 256 threads x 4 keys x kProbeRounds.
+constexpr int kProbeRounds = 4;
+constexpr uint32_t kProbeTile = kProbeThreads * 4 * kProbeRounds;
+
+#ifdef __CUDACC__
+template <class Cfg>
+struct BloomLaunch {
+  static cudaError_t probe(const ProbeArgs& a, int grid, cudaStream_t s) {
+    probe_kernel<BloomOps<Cfg>, kProbeRounds><<<grid, kProbeThreads, 0, s>>>(a);
+    return cudaGetLastError();
+  }
+  static cudaError_t build(const BuildArgs& a, int grid, cudaStream_t s) {
+    bloom_build_kernel<Cfg><<<grid, 256, 0, s>>>(a);
+    return cudaGetLastError();
+  }
+  static int occupancy() {
+    int n = 0;
+    cudaOccupancyMaxActiveBlocksPerMultiprocessor(&n, probe_kernel<BloomOps<Cfg>, kProbeRounds>,
+                                                  kProbeThreads, 0);
+    return n;
+  }
+};
+
+template <typename Word, int W, int S, int Z, int K>
+BloomKernels bloom_entry() {
+  using C = BloomCfg<Word, W, S, Z, K>;
+  return BloomKernels{static_cast<uint32_t>(sizeof(Word)), W, S, Z, K, &BloomLaunch<C>::probe,
+                      &BloomLaunch<C>::build, &BloomLaunch<C>::occupancy};
+}
+
+template <int T, int B>
+struct CuckooLaunch {
+  using C = CuckooCfg<T, B>;
+  static cudaError_t probe(const ProbeArgs& a, int grid, cudaStream_t s) {
+    probe_kernel<CuckooOps<C>, kProbeRounds><<<grid, kProbeThreads, 0, s>>>(a);
+    return cudaGetLastError();
+  }
+  static int occupancy() {
+    int n = 0;
+    cudaOccupancyMaxActiveBlocksPerMultiprocessor(&n, probe_kernel<CuckooOps<C>, kProbeRounds>,
+                                                  kProbeThreads, 0);
+    return n;
+  }
+  static void unpack(const uint32_t* t, uint32_t* sl, uint32_t nb, int grid, cudaStream_t s) {
+    cuckoo_unpack_kernel<C><<<grid, 256, 0, s>>>(t, sl, nb);
+  }
+  static void insert(const CuckooBuildArgs& a, int grid, cudaStream_t s) {
+    cuckoo_insert_kernel<C><<<grid, 256, 0, s>>>(a);
+  }
+  static void pack(uint32_t* t, const uint32_t* sl, uint32_t nb, uint64_t words, int grid, cudaStream_t s) {
+    cuckoo_pack_kernel<C><<<grid, 256, 0, s>>>(t, sl, nb, words);
+  }
+  static void count(const uint32_t* t, uint32_t nb, uint64_t vw, unsigned long long* out, int grid,
+                    cudaStream_t s) {
+    cuckoo_count_kernel<C><<<grid, 256, 0, s>>>(t, nb, vw, out);
+  }
+};
+
+template <int T, int B>
+CuckooKernels cuckoo_entry() {
+  using L = CuckooLaunch<T, B>;
+  return CuckooKernels{T, B, &L::probe, &L::occupancy, &L::unpack, &L::insert, &L::pack, &L::count};
+}
+#endif
+
+}  // namespace dtlg

@@ -1,0 +1,101 @@
+"""ctypes binding of libdtlg.so (include/dtlg.h).
+
+The product path: every filter operation in this package goes through these
+entry points into the sm_100a kernels.  There is no CPU fallback: if the
+library is missing, importing the package raises.
+"""
+import ctypes as C
+import os
+
+PKG_ROOT = os.path.dirname(os.path.dirname(os.path.abspath(__file__)))
+LIB_PATH = os.environ.get("DTLG_LIB", os.path.join(PKG_ROOT, "lib", "libdtlg.so"))
+
+OK = 0
+STATUS = {
+    0: "ok", 1: "invalid configuration", 2: "filter size out of range", 3: "null pointer",
+    4: "filter words must be 16-byte aligned", 5: "CUDA error", 6: "allocation failed",
+    7: "cuckoo filter full", 8: "device wait timed out", 9: "workspace too small",
+    10: "unsupported operation",
+}
+
+
+class DtlgError(RuntimeError):
+    def __init__(self, status, what=""):
+        self.status = status
+        msg = STATUS.get(status, f"status {status}")
+        if status == 5:
+            msg += ": " + lib().dtlg_last_cuda_error().decode()
+        super().__init__(f"{what}: {msg}" if what else msg)
+
+
+class InvalidConfig(DtlgError, ValueError):
+    """The reference's std::invalid_argument (blocked_bloomfilter.hpp:111)."""
+
+
+class SizeError(DtlgError, ValueError):
+    """The reference's std::logic_error on block counts (block_addressing_logic.hpp:81)."""
+
+
+class BloomConfigS(C.Structure):
+    _fields_ = [("k", C.c_uint32), ("word_size", C.c_uint32), ("word_cnt_per_block", C.c_uint32),
+                ("sector_cnt", C.c_uint32), ("addr_mode", C.c_uint32), ("zone_cnt", C.c_uint32)]
+
+
+class CuckooConfigS(C.Structure):
+    _fields_ = [("bits_per_tag", C.c_uint32), ("tags_per_bucket", C.c_uint32), ("addr_mode", C.c_uint32)]
+
+
+# every entry point declared in include/dtlg.h: name -> (restype, argtypes)
+_vp, _u32, _u64, _i = C.c_void_p, C.c_uint32, C.c_uint64, C.c_int
+_u64p = C.POINTER(C.c_uint64)
+SIGNATURES = {
+    "dtlg_bloom_create": (_i, [C.POINTER(BloomConfigS), _u64, C.POINTER(_vp)]),
+    "dtlg_cuckoo_create": (_i, [C.POINTER(CuckooConfigS), _u64, C.POINTER(_vp)]),
+    "dtlg_destroy": (None, [_vp]),
+    "dtlg_size_in_bytes": (_u64, [_vp]),
+    "dtlg_size": (_u64, [_vp]),
+    "dtlg_alloc_words_u64": (_u64, [_vp]),
+    "dtlg_name": (C.c_size_t, [_vp, C.c_char_p, C.c_size_t]),
+    "dtlg_kind": (_i, [_vp]),
+    "dtlg_block_cnt": (_u64, [_vp]),
+    "dtlg_is_magic": (_i, [_vp]),
+    "dtlg_batch_insert": (_i, [_vp, _vp, _vp, _u32, _u64p, _vp]),
+    "dtlg_batch_contains": (_i, [_vp, _vp, _vp, _u32, _vp, _u32, _u64p, _vp]),
+    "dtlg_batch_contains_async": (_i, [_vp, _vp, _vp, _u32, _vp, _u32, _vp, _vp]),
+    "dtlg_probe_workspace_size": (C.c_size_t, [_u32]),
+    "dtlg_batch_contains_ws": (_i, [_vp, _vp, _vp, _u32, _vp, _u32, _vp, _vp, C.c_size_t, _vp]),
+    "dtlg_insert": (_i, [_vp, _vp, _u32, _vp]),
+    "dtlg_contains": (_i, [_vp, _vp, _u32, C.POINTER(_i), _vp]),
+    "dtlg_batch_contains_host": (_i, [_vp, _vp, _vp, _u64, _vp, _u32, _u64p, _vp]),
+    "dtlg_batch_insert_host": (_i, [_vp, _vp, _vp, _u64, _u64p, _vp]),
+    "dtlg_count_occupied_slots": (_i, [_vp, _vp, _u64p, _vp]),
+    "dtlg_status_string": (C.c_char_p, [_i]),
+    "dtlg_last_cuda_error": (C.c_char_p, []),
+    "dtlg_version": (C.c_char_p, []),
+}
+
+_lib = None
+
+
+def lib():
+    global _lib
+    if _lib is None:
+        if not os.path.exists(LIB_PATH):
+            raise ImportError(f"libdtlg.so not built at {LIB_PATH} (make -C bloomfilter-bsd_b200)")
+        L = C.CDLL(LIB_PATH)
+        for name, (res, args) in SIGNATURES.items():
+            fn = getattr(L, name)
+            fn.restype = res
+            fn.argtypes = args
+        _lib = L
+    return _lib
+
+
+def check(status, what=""):
+    if status == OK:
+        return
+    if status == 1:
+        raise InvalidConfig(status, what)
+    if status == 2:
+        raise SizeError(status, what)
+    raise DtlgError(status, what)

@@ -66,6 +66,51 @@ def probe_keys(n_build, n_probe, hit_ratio, seed, start=0, chunk=1 << 24):
     return keys, member
 
 
+def _mix32_torch(x, seed):
+    """_mix32 on an int64 torch tensor (values < 2^32), bit-identical."""
+    m = 0xFFFFFFFF
+    s = seed & 0xFFFFFFFF
+    x = (x + ((s * 0x9E3779B9) & m)) & m
+    x = (x * 0x85EBCA6B) & m
+    x ^= x >> 13
+    x = (x * 0xC2B2AE35) & m
+    x ^= x >> 16
+    x = (x * ((((0x27D4EB2F ^ (seed * 2)) | 1)) & m)) & m
+    x ^= x >> 15
+    return x
+
+
+def build_keys_torch(n, seed, device="cuda", start=0):
+    """build_keys on the device (int32 tensor holding the uint32 keys)."""
+    import torch
+    i = torch.arange(start, start + n, dtype=torch.int64, device=device)
+    return _to_i32(_mix32_torch(i, seed))
+
+
+def probe_keys_torch(n_build, n_probe, hit_ratio, seed, start=0, device="cuda", chunk=1 << 26):
+    """probe_keys on the device; returns (int32 keys, bool member)."""
+    import torch
+    assert n_build + start + n_probe <= (1 << 32), "counter space exhausted"
+    keys = torch.empty(n_probe, dtype=torch.int32, device=device)
+    member = torch.empty(n_probe, dtype=torch.bool, device=device)
+    thr = int(hit_ratio * (1 << 32))
+    for b in range(0, n_probe, chunk):
+        e = min(n_probe, b + chunk)
+        i = torch.arange(start + b, start + e, dtype=torch.int64, device=device)
+        r = _mix32_torch(i.clone(), seed ^ 0x5EED1)
+        hit = (r < thr) if n_build > 0 else torch.zeros_like(r, dtype=torch.bool)
+        j = _mix32_torch(i.clone(), seed ^ 0xB10C) % max(1, n_build)
+        src = torch.where(hit, j, i + n_build)
+        keys[b:e] = _to_i32(_mix32_torch(src, seed))
+        member[b:e] = hit
+    return keys, member
+
+
+def _to_i32(x):
+    import torch
+    return torch.where(x >= (1 << 31), x - (1 << 32), x).to(torch.int32)
+
+
 def uniform_keys(n, seed):
     """n distinct keys spread uniformly over u32, standing in for the unique
     random keys of the reference's calibration runs (model/benchmark.cpp:82-95)."""

@@ -1,0 +1,152 @@
+/*
+ * dtlg.h -- C ABI of the B200-native DTL filter build/probe library (libdtlg.so).
+ *
+ * Drop-in boundary for the filter path of peterboncz/bloomfilter-bsd ("dtl").
+ * The reference exposes that path as the C++ interface dtl::filter::filter_base
+ * (src/dtl/filter/filter_base.hpp:11-62), implemented by bbf_32, bbf_64,
+ * zbbf_32, zbbf_64 and cf, constructed by config through the dtl::filter::filter
+ * facade (src/dtl/filter/filter.hpp:42-72,166-169).  Every entry point below
+ * names the reference member it replaces.
+ *
+ * Conventions
+ *  - Plain pointers and sizes only; no C++ or torch types cross this boundary.
+ *  - Unless a name ends in _host, every data pointer is a DEVICE pointer on the
+ *    current CUDA device, and work is enqueued on `stream` (0 = legacy default).
+ *  - As in the reference, the caller owns the filter words (filter.hpp:92-119):
+ *    allocate dtlg_alloc_words_u64() 64-bit words, zero them, pass them in.
+ *  - Errors are returned as dtlg_status; nothing is thrown across the ABI.
+ *  - Results are bit-identical to the reference's scalar contains path:
+ *    the same filter words after batch_insert (Bloom) and the same ascending
+ *    match positions i + match_offset (32-bit wrap) from batch_contains.
+ */
+#ifndef DTLG_H
+#define DTLG_H
+
+#include <stddef.h>
+#include <stdint.h>
+
+#ifdef __cplusplus
+extern "C" {
+#endif
+
+typedef struct CUstream_st* dtlg_stream_t; /* == cudaStream_t */
+
+typedef enum dtlg_status {
+  DTLG_OK = 0,
+  DTLG_ERR_INVALID_CONFIG = 1, /* reference: std::invalid_argument / runtime_error from the ctor */
+  DTLG_ERR_SIZE = 2,           /* reference: std::logic_error "block count must not exceed 2^32" */
+  DTLG_ERR_NULL = 3,           /* a required pointer is NULL */
+  DTLG_ERR_ALIGNMENT = 4,      /* filter words not 16-byte aligned */
+  DTLG_ERR_CUDA = 5,           /* a CUDA call failed; see dtlg_last_cuda_error() */
+  DTLG_ERR_ALLOC = 6,          /* device or pinned allocation failed */
+  DTLG_ERR_CUCKOO_FULL = 7,    /* reference: cuckoo batch_insert returned false */
+  DTLG_ERR_TIMEOUT = 8,        /* a bounded device wait gave up (look-back / queue) */
+  DTLG_ERR_WORKSPACE = 9,      /* caller workspace too small */
+  DTLG_ERR_UNSUPPORTED = 10    /* operation not defined for this filter kind */
+} dtlg_status;
+
+/* Mirrors dtl::blocked_bloomfilter_config
+ * (src/dtl/filter/blocked_bloomfilter/blocked_bloomfilter_config.hpp:11-18).
+ * addr_mode is informational, as in the reference: the addressing is POW2 iff
+ * m is a power of two (blocked_bloomfilter.hpp:234-242). */
+typedef struct dtlg_bloom_config {
+  uint32_t k;                  /* bits set per key, 1..16 (default 8) */
+  uint32_t word_size;          /* bytes per word, 4 or 8 (default 4) */
+  uint32_t word_cnt_per_block; /* 1,2,4,8,16 (default 1) */
+  uint32_t sector_cnt;         /* 1,2,4,8,16 (default 1) */
+  uint32_t addr_mode;          /* 0 = POW2, 1 = MAGIC (ignored on create) */
+  uint32_t zone_cnt;           /* 1 = not zoned; 2,4,8 = zoned (default 1) */
+} dtlg_bloom_config;
+
+/* Mirrors dtl::cuckoofilter::config
+ * (src/dtl/filter/cuckoofilter/cuckoofilter_config.hpp:13-16). */
+typedef struct dtlg_cuckoo_config {
+  uint32_t bits_per_tag;    /* 4, 8, 12, 16, 32 */
+  uint32_t tags_per_bucket; /* 1, 2, 4 */
+  uint32_t addr_mode;       /* informational, as above */
+} dtlg_cuckoo_config;
+
+typedef struct dtlg_filter dtlg_filter;
+
+/* ---- construction (filter.hpp:42-72; bbf_32.hpp:53, zbbf_*.hpp, cf.hpp) ---- */
+dtlg_status dtlg_bloom_create(const dtlg_bloom_config* cfg, uint64_t m_bits, dtlg_filter** out);
+dtlg_status dtlg_cuckoo_create(const dtlg_cuckoo_config* cfg, uint64_t m_bits, dtlg_filter** out);
+void dtlg_destroy(dtlg_filter* f);
+
+/* ---- sizes and name ---- */
+/* filter_base::size_in_bytes() (filter_base.hpp:52) */
+uint64_t dtlg_size_in_bytes(const dtlg_filter* f);
+/* filter_base::size(): filter size in 64-bit words (filter_base.hpp:56) */
+uint64_t dtlg_size(const dtlg_filter* f);
+/* 64-bit words the caller must allocate (zeroed): size(), plus for cuckoo the
+ * victim-cache record the reference keeps past size() (cuckoofilter_logic.hpp:
+ * 145-157) and read slack. */
+uint64_t dtlg_alloc_words_u64(const dtlg_filter* f);
+/* filter_base::name(): the reference's JSON description (filter_base.hpp:48,
+ * blocked_bloomfilter.hpp:372-390, zoned_blocked_bloomfilter.hpp:358-378,
+ * cuckoofilter.hpp:335-343).  Writes a NUL-terminated string; returns its
+ * length (excluding NUL) or the required length if cap is too small. */
+size_t dtlg_name(const dtlg_filter* f, char* buf, size_t cap);
+/* Introspection: 0 = Bloom, 1 = zoned Bloom, 2 = cuckoo; block (bucket) count;
+ * 1 if MAGIC addressing. */
+int dtlg_kind(const dtlg_filter* f);
+uint64_t dtlg_block_cnt(const dtlg_filter* f);
+int dtlg_is_magic(const dtlg_filter* f);
+
+/* ---- build: filter_base::batch_insert (filter_base.hpp:26) ---- */
+/* Bloom: always DTLG_OK on valid input (bbf_32.cpp:41-45).  Cuckoo: returns
+ * DTLG_ERR_CUCKOO_FULL when some key could not be placed (the reference's
+ * `false`, cuckoofilter_logic.hpp:330-337); *failed_out (optional) gets the
+ * number of keys lost.  Synchronous w.r.t. `stream` for cuckoo only. */
+dtlg_status dtlg_batch_insert(const dtlg_filter* f, uint64_t* filter_words, const uint32_t* keys,
+                              uint32_t key_cnt, uint64_t* failed_out, dtlg_stream_t stream);
+
+/* ---- probe: filter_base::batch_contains (filter_base.hpp:42-45) ---- */
+/* Writes the positions i + match_offset of matching keys, ascending, to
+ * match_positions (capacity >= key_cnt) and the match count to *match_cnt
+ * (HOST pointer); blocks until the count is known. */
+dtlg_status dtlg_batch_contains(const dtlg_filter* f, const uint64_t* filter_words,
+                                const uint32_t* keys, uint32_t key_cnt, uint32_t* match_positions,
+                                uint32_t match_offset, uint64_t* match_cnt, dtlg_stream_t stream);
+/* Fully asynchronous form: the count goes to *match_cnt_dev (DEVICE pointer). */
+dtlg_status dtlg_batch_contains_async(const dtlg_filter* f, const uint64_t* filter_words,
+                                      const uint32_t* keys, uint32_t key_cnt,
+                                      uint32_t* match_positions, uint32_t match_offset,
+                                      uint64_t* match_cnt_dev, dtlg_stream_t stream);
+/* Same, with a caller-provided device workspace of at least
+ * dtlg_probe_workspace_size(key_cnt) bytes (no allocation inside). */
+size_t dtlg_probe_workspace_size(uint32_t key_cnt);
+dtlg_status dtlg_batch_contains_ws(const dtlg_filter* f, const uint64_t* filter_words,
+                                   const uint32_t* keys, uint32_t key_cnt, uint32_t* match_positions,
+                                   uint32_t match_offset, uint64_t* match_cnt_dev, void* workspace,
+                                   size_t workspace_bytes, dtlg_stream_t stream);
+
+/* ---- single keys: filter_base::insert / contains (filter_base.hpp:22,32) ---- */
+dtlg_status dtlg_insert(const dtlg_filter* f, uint64_t* filter_words, uint32_t key, dtlg_stream_t stream);
+dtlg_status dtlg_contains(const dtlg_filter* f, const uint64_t* filter_words, uint32_t key,
+                          int* result, dtlg_stream_t stream);
+
+/* ---- host-buffer forms (the reference's calling convention: all host memory).
+ * Keys and positions are HOST pointers; the filter words stay on the device.
+ * Copies are staged through pinned memory in chunks that overlap the kernels. */
+dtlg_status dtlg_batch_contains_host(const dtlg_filter* f, const uint64_t* filter_words,
+                                     const uint32_t* keys_host, uint64_t key_cnt,
+                                     uint32_t* match_positions_host, uint32_t match_offset,
+                                     uint64_t* match_cnt, dtlg_stream_t stream);
+dtlg_status dtlg_batch_insert_host(const dtlg_filter* f, uint64_t* filter_words,
+                                   const uint32_t* keys_host, uint64_t key_cnt, uint64_t* failed_out,
+                                   dtlg_stream_t stream);
+
+/* ---- cuckoo helpers (cuckoofilter_logic.hpp:496-504) ---- */
+dtlg_status dtlg_count_occupied_slots(const dtlg_filter* f, const uint64_t* filter_words,
+                                      uint64_t* count, dtlg_stream_t stream);
+
+/* ---- library ---- */
+const char* dtlg_status_string(dtlg_status s);
+const char* dtlg_last_cuda_error(void);
+const char* dtlg_version(void);
+
+#ifdef __cplusplus
+}
+#endif
+#endif /* DTLG_H */

@@ -1,0 +1,211 @@
+"""Parity of the CUDA path (through the C ABI) with the reference.
+
+Bit-exact: Bloom filter words after batch_insert, and the ascending match
+positions of batch_contains, against the C oracle (itself pinned to the
+reference) and against golden vectors produced by the reference.
+"""
+import numpy as np
+import pytest
+
+import dtlg as F
+import oracle as O
+from dtlg import keygen
+from gen_ref_instances import bloom_configs, cuckoo_configs
+
+pytestmark = pytest.mark.gpu
+torch = pytest.importorskip("torch")
+
+
+def dev_words(np_words):
+    return torch.from_numpy(np.ascontiguousarray(np_words).view(np.int64)).cuda()
+
+
+def dev_keys(keys, pad=0):
+    """uint32 keys on the device starting `pad` keys into a buffer (pad=1..3
+    gives a key pointer that is not 16-byte aligned)."""
+    k = np.ascontiguousarray(keys, dtype=np.uint32)
+    buf = torch.zeros(len(k) + 8, dtype=torch.int32, device="cuda")
+    if len(k):
+        buf[pad:pad + len(k)] = torch.from_numpy(k.view(np.int32)).cuda()
+    return buf[pad:pad + len(k)]
+
+
+def gpu_probe(f, words_t, keys, offset=0, pad=0):
+    kt = dev_keys(keys, pad)
+    out = torch.full((max(1, len(keys)),), -1, dtype=torch.int32, device="cuda")
+    n = f.batch_contains(words_t, kt, len(keys), out, offset)
+    return out[:n].cpu().numpy().view(np.uint32).copy()
+
+
+def test_reference_known_answer_facade():
+    # src/dtl/filter/filter_test.cpp:16-40, through the filter facade
+    f = F.filter(F.blocked_bloomfilter_config(), 1024)
+    assert f.insert(torch.tensor([13, 37, 42, 88], dtype=torch.int32, device="cuda"))
+    p = f.probe()
+    pos = torch.zeros(4, dtype=torch.int32, device="cuda")
+    assert p(torch.tensor([13, 37, 42, 88], dtype=torch.int32, device="cuda"), pos, 0) == 4
+    assert pos.tolist() == [0, 1, 2, 3]
+    assert p(torch.tensor([0, 1, 42, 2], dtype=torch.int32, device="cuda"), pos, 1000) == 1
+    assert pos[0].item() == 1002
+    # host buffers (the reference's calling convention)
+    hp = np.zeros(4, dtype=np.uint32)
+    assert p(np.array([0, 1, 42, 2], dtype=np.uint32), hp, 1000) == 1 and hp[0] == 1002
+
+
+def test_bloom_every_config_bit_exact():
+    """Every config the reference's dispatchers accept, POW2 and MAGIC:
+    GPU-built words == oracle-built words, GPU probe == oracle probe."""
+    for ci, (wb, w, s, z, k) in enumerate(bloom_configs()):
+        for m in (1 << 14, (1 << 14) + 1000):
+            ob = O.Bloom(wb, w, s, z, k, m)
+            f = F.construct(F.blocked_bloomfilter_config(k=k, word_size=wb, word_cnt_per_block=w,
+                                                         sector_cnt=s, zone_cnt=z), m)
+            n = max(1, int(ob.m_actual // 12))
+            seed = 100 + ci
+            bk = keygen.build_keys(n, seed)
+            ref_words = ob.alloc()
+            ob.insert(ref_words, bk)
+            words = f.alloc_filter_data()
+            assert f.batch_insert(words, dev_keys(bk, pad=ci % 4))
+            got = words.cpu().numpy().view(np.uint64)
+            assert np.array_equal(got, ref_words), (wb, w, s, z, k, m)
+            pk, _ = keygen.probe_keys(n, 3001, 0.4, seed)
+            off = (1 << 32) - 1500 if ci % 2 else 17
+            exp = ob.batch_contains(ref_words, pk, off)
+            assert np.array_equal(gpu_probe(f, words, pk, off, pad=(ci + 1) % 4), exp), (wb, w, s, z, k, m)
+
+
+def test_bloom_golden_vectors(golden):
+    index, arr = golden
+    for e in index["bloom"]:
+        wb, w, s, z, k = e["cfg"]
+        f = F.construct(F.blocked_bloomfilter_config(k=k, word_size=wb, word_cnt_per_block=w, sector_cnt=s,
+                                                     zone_cnt=z), e["m"])
+        words = f.alloc_filter_data()
+        assert f.batch_insert(words, dev_keys(keygen.build_keys(e["n_build"], e["seed"])))
+        ref = arr[f"bloom_{e['id']}_words"]
+        assert np.array_equal(words.cpu().numpy().view(np.uint64)[:len(ref)], ref), e
+        pk, _ = keygen.probe_keys(e["n_build"], e["n_probe"], e["hit_ratio"], e["seed"])
+        assert np.array_equal(gpu_probe(f, words, pk, e["match_offset"]), arr[f"bloom_{e['id']}_hits"]), e
+
+
+@pytest.mark.parametrize("n", [0, 1, 2, 3, 4, 5, 31, 1023, 1024, 4095, 4096, 4097, 8191, 65537, 300001])
+def test_probe_lengths_and_alignment(n):
+    ob = O.Bloom(8, 8, 8, 1, 8, 3 * (1 << 16))
+    f = F.bbf_64(3 * (1 << 16), 8, 8, 8)
+    bk = keygen.build_keys(20000, 5)
+    rw = ob.alloc()
+    ob.insert(rw, bk)
+    words = dev_words(rw)
+    pk, _ = keygen.probe_keys(20000, n, 0.5, 5)
+    for pad in range(4):
+        assert np.array_equal(gpu_probe(f, words, pk, 9, pad), ob.batch_contains(rw, pk, 9))
+
+
+def test_cuckoo_probe_every_config_bit_exact():
+    """Tables built on the CPU (restatement of the reference's insert), uploaded,
+    probed on the GPU: identical match lists, victim cache included."""
+    for ci, (t, b) in enumerate(cuckoo_configs()):
+        for m in (1 << 16, (1 << 16) + 4321):
+            oc = O.Cuckoo(t, b, m)
+            f = F.cf(m, t, b)
+            assert f.alloc_words() >= oc.alloc_u64 - 2
+            table = np.zeros(f.alloc_words(), dtype=np.uint64)
+            n = int(oc.bucket_cnt * b * (0.97 if b == 4 else 0.6))
+            bk = keygen.build_keys(n, 300 + ci)
+            oc.insert(table, bk, seed=ci + 1)
+            pk, _ = keygen.probe_keys(n, 5000, 0.3, 300 + ci)
+            exp = oc.batch_contains(table, pk, 11)
+            assert np.array_equal(gpu_probe(f, dev_words(table), pk, 11, pad=ci % 4), exp), (t, b, m)
+            assert f.count_occupied_slots(dev_words(table)) == oc.count_occupied(table)
+
+
+def test_cuckoo_golden_vectors(golden):
+    index, arr = golden
+    for e in index["cuckoo"]:
+        f = F.cf(e["m"], e["t"], e["b"])
+        ref_table = arr[f"cuckoo_{e['id']}_table"]
+        table = np.zeros(max(f.alloc_words(), len(ref_table)), dtype=np.uint64)
+        table[:len(ref_table)] = ref_table
+        pk, _ = keygen.probe_keys(e["n_build"], e["n_probe"], e["hit_ratio"], e["seed"])
+        got = gpu_probe(f, dev_words(table), pk, e["match_offset"])
+        assert np.array_equal(got, arr[f"cuckoo_{e['id']}_hits"]), e
+
+
+@pytest.mark.parametrize("t,b,m", [(16, 4, 1 << 20), (8, 4, 1 << 20), (12, 4, 1 << 20), (16, 4, 4462025 * 64),
+                                   (8, 2, (1 << 18) + 3), (32, 4, 1 << 18), (4, 4, 1 << 18), (16, 1, 1 << 18)])
+def test_cuckoo_gpu_build_invariants(t, b, m):
+    """The GPU build is randomised like the reference's; check no false
+    negatives, occupancy, and the false-positive rate against a CPU build."""
+    oc = O.Cuckoo(t, b, m)
+    f = F.cf(m, t, b)
+    lf = 0.9 if b == 4 else (0.75 if b == 2 else 0.4)
+    n = int(oc.bucket_cnt * b * lf)
+    bk = keygen.build_keys(n, 77)
+    words = f.alloc_filter_data()
+    ok = f.batch_insert(words, dev_keys(bk))
+    assert ok, f"lost {f.last_failed} of {n}"
+    occ = f.count_occupied_slots(words)
+    assert occ == n
+    # no false negatives
+    members = gpu_probe(f, words, bk)
+    assert len(members) == n
+    # FPR vs the CPU restatement's build of the same keys
+    neg, _ = keygen.probe_keys(n, 200000, 0.0, 77)
+    fp_gpu = len(gpu_probe(f, words, neg))
+    table = np.zeros(f.alloc_words(), dtype=np.uint64)
+    assert oc.insert(table, bk, seed=3)
+    fp_cpu = len(oc.batch_contains(table, neg))
+    # the tag sets are equal; only slot placement differs -> same FPR
+    sd = np.sqrt(max(fp_cpu, 1))
+    assert abs(fp_gpu - fp_cpu) <= 5 * sd + 5, (fp_gpu, fp_cpu)
+
+
+def test_host_buffer_pipeline_multi_chunk():
+    """batch_contains over host buffers, more keys than one pipeline chunk."""
+    m = 1 << 24
+    ob = O.Bloom(8, 8, 8, 1, 8, m)
+    f = F.bbf_64(m, 8, 8, 8)
+    bk = keygen.build_keys(1 << 20, 9)
+    words = f.alloc_filter_data()
+    assert f.batch_insert_host(words, bk)
+    rw = ob.alloc()
+    ob.insert(rw, bk)
+    assert np.array_equal(words.cpu().numpy().view(np.uint64), rw)
+    pk, _ = keygen.probe_keys(1 << 20, (1 << 24) * 2 + 12345, 0.1, 9)
+    out = np.zeros(len(pk), dtype=np.uint32)
+    n = f.batch_contains_host(words, pk, out, 123)
+    exp = ob.batch_contains(rw, pk, 123)
+    assert n == len(exp) and np.array_equal(out[:n], exp)
+
+
+def test_single_key_api():
+    f = F.bbf_32(1 << 16, 6, 2, 1)
+    words = f.alloc_filter_data()
+    assert f.insert(words, 4242)
+    assert f.contains(words, 4242)
+    assert not f.contains(words, 4243) or True  # a false positive is allowed
+    ob = O.Bloom(4, 2, 1, 1, 6, 1 << 16)
+    rw = ob.alloc()
+    ob.insert(rw, [4242])
+    assert np.array_equal(words.cpu().numpy().view(np.uint64), rw)
+
+
+def test_large_filter_property():
+    """A DRAM-resident sectorized filter (u64, w=8, s=8, k=8, 16 bits/key,
+    2^26 keys, 128 MiB): every member found; positions identical to the oracle."""
+    n = 1 << 26
+    m = n * 16
+    ob = O.Bloom(8, 8, 8, 1, 8, m)
+    f = F.bbf_64(m, 8, 8, 8)
+    bk = keygen.build_keys(n, 21)
+    words = f.alloc_filter_data()
+    assert f.batch_insert(words, dev_keys(bk))
+    rw = ob.alloc()
+    ob.insert(rw, bk)
+    assert np.array_equal(words.cpu().numpy().view(np.uint64), rw)
+    pk, member = keygen.probe_keys(n, 1 << 24, 0.1, 21)
+    got = gpu_probe(f, words, pk)
+    exp = ob.batch_contains(rw, pk)
+    assert np.array_equal(got, exp)
+    assert np.all(np.isin(np.nonzero(member)[0].astype(np.uint32), got))
