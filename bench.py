@@ -33,6 +33,9 @@ WORKLOADS = {
     # name: (word_size, w, s, z, k, log2 n, bits/key, log2 probes, hit ratio)
     "sectorized_dram": (8, 8, 8, 1, 8, 28, 16, 28, 0.10),
     "sectorized_l2": (8, 8, 8, 1, 8, 22, 16, 28, 0.10),
+    # the same filter type at 2^27 keys (256 MiB, still DRAM-resident) with
+    # 2^26 probes: the case ncu captures run on
+    "sectorized_dram_small": (8, 8, 8, 1, 8, 27, 16, 26, 0.10),
     "register_blocked": (4, 1, 1, 1, 4, 20, 16, 24, 0.10),
 }
 SEED = 20240601
