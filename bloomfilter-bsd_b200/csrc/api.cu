@@ -9,16 +9,11 @@
 #include <vector>
 
 #include "../../include/dtlg.h"
+#include "filter_handle.hpp"
 #include "host_config.hpp"
 #include "registry.hpp"
 
 using namespace dtlg;
-
-struct dtlg_filter {
-  FilterDesc d;
-  const BloomKernels* bk = nullptr;
-  const CuckooKernels* ck = nullptr;
-};
 
 namespace dtlg {
 

@@ -121,6 +121,24 @@ dtlg_status dtlg_batch_contains_ws(const dtlg_filter* f, const uint64_t* filter_
                                    uint32_t match_offset, uint64_t* match_cnt_dev, void* workspace,
                                    size_t workspace_bytes, dtlg_stream_t stream);
 
+/* ---- probe without any allocation (no counterpart in the reference) ----
+ * For callers that cannot call cudaMalloc -- a query engine whose device
+ * memory is all owned by its own buffer manager, a plugin inside a host
+ * application that has claimed the GPU's memory, a latency-critical path that
+ * cannot afford an allocation's synchronization.  Same result as
+ * dtlg_batch_contains_async; the count goes to *match_cnt_dev (DEVICE).  The
+ * probe's scratch (tile queue + look-back words) lives in one static device
+ * array of about 128 KiB per GPU, held until exit; key_cnt above
+ * DTLG_NOALLOC_MAX_KEYS is rejected with DTLG_ERR_WORKSPACE.  The first call
+ * on each device looks the array's address up (make that first call before
+ * any stream capture).  All calls share the array: calls that overlap on the
+ * GPU race and must be serialized by the caller. */
+#define DTLG_NOALLOC_MAX_KEYS (1u << 26)
+dtlg_status dtlg_batch_contains_noalloc(const dtlg_filter* f, const uint64_t* filter_words,
+                                        const uint32_t* keys, uint32_t key_cnt,
+                                        uint32_t* match_positions, uint32_t match_offset,
+                                        uint64_t* match_cnt_dev, dtlg_stream_t stream);
+
 /* ---- single keys: filter_base::insert / contains (filter_base.hpp:22,32) ---- */
 dtlg_status dtlg_insert(const dtlg_filter* f, uint64_t* filter_words, uint32_t key, dtlg_stream_t stream);
 dtlg_status dtlg_contains(const dtlg_filter* f, const uint64_t* filter_words, uint32_t key,
