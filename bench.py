@@ -44,7 +44,7 @@ SEED = 20240601
 def parse():
     ap = argparse.ArgumentParser()
     ap.add_argument("--gpus", type=int, default=1)
-    ap.add_argument("--steps", type=int, default=20)
+    ap.add_argument("--steps", type=int, default=100)
     ap.add_argument("--warmup", type=int, default=5)
     ap.add_argument("--impl", choices=("dtlg", "reference"), default="dtlg")
     ap.add_argument("--workload", choices=sorted(WORKLOADS), default="sectorized_dram")
@@ -219,6 +219,8 @@ def run_dtlg(args):
         if st:
             raise RuntimeError(f"dtlg_batch_contains_ws failed: {st}")
 
+    clocks = ClockSampler(local)
+    clocks.start()
     for _ in range(max(3, args.warmup)):
         step()
     torch.cuda.synchronize()
@@ -228,8 +230,6 @@ def run_dtlg(args):
     if world > 1:
         dist.barrier()
     torch.cuda.synchronize()
-    clocks = ClockSampler(local)
-    clocks.start()
     evs = [(torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)) for _ in range(args.steps)]
     t_start = torch.cuda.Event(enable_timing=True)
     t_end = torch.cuda.Event(enable_timing=True)
@@ -277,7 +277,8 @@ def run_dtlg(args):
                      "peak_source": f"MEASURED_PEAKS.json hbm_gbs ({peak_kind})",
                      "algorithmic_bytes_per_key": round(alg_bytes_per_key, 3),
                      "dram_resident": dram_resident},
-        "gpu_launches": args.steps,
+        "gpu_launches": args.steps * L.dtlg_probe_kernel_count(f._h, P),
+        "kernels_per_step": L.dtlg_probe_kernel_count(f._h, P),
         "match_count_per_gpu": count,
         "clocks": clk,
     }
@@ -319,7 +320,7 @@ def run_dtlg(args):
                          "ms_per_step": round(e_ms, 3), "h2d_bytes_per_step": P * 4,
                          "d2h_bytes_per_step": count * 4 + 8 * chunks,
                          "api": "dtlg_batch_contains_host (pinned host keys -> host positions)"}
-        result["gpu_launches"] += e_steps * chunks
+        result["gpu_launches"] += e_steps * chunks * L.dtlg_probe_kernel_count(f._h, 1 << 24)
 
     # the reference's CPU path on this host, bounded sample (rank 0, N=1 only)
     if rank == 0 and world == 1 and not args.no_cpu_baseline:

@@ -99,6 +99,43 @@ static_assert(sizeof(WsHeader) == 128, "header is one 128-byte line");
 
 uint32_t probe_tiles(uint64_t n_phys) { return static_cast<uint32_t>((n_phys + kProbeTile - 1) / kProbeTile); }
 
+// Two-pass layout inside the same workspace: header | status words | bitmask.
+constexpr uint64_t kTwoPassMinKeys = 1ull << 20;
+uint64_t bits_words(uint64_t n_phys) { return (n_phys + 31) / 32; }
+uint32_t compact_tiles(uint64_t n_phys) {
+  return static_cast<uint32_t>((bits_words(n_phys) + kCompactTileWords - 1) / kCompactTileWords);
+}
+size_t status_bytes(uint64_t n_phys) {
+  const uint64_t t = std::max<uint64_t>(probe_tiles(n_phys), compact_tiles(n_phys));
+  return static_cast<size_t>(((t * 8 + 255) / 256) * 256);
+}
+size_t workspace_bytes(uint64_t n_phys) {
+  return sizeof(WsHeader) + status_bytes(n_phys) + static_cast<size_t>(((bits_words(n_phys) * 4 + 255) / 256) * 256);
+}
+
+int compact_occupancy() {
+  static int occ = [] {
+    int n = 0;
+    cudaOccupancyMaxActiveBlocksPerMultiprocessor(&n, compact_kernel, kCompactThreads, 0);
+    return std::max(1, n);
+  }();
+  return occ;
+}
+
+// Block-range passes of the two-pass probe.  Random probes over more than
+// ~256 MiB of filter run out of the GPU's address-translation reach (B200: the
+// probe rate falls from ~62 to ~25 Gkeys/s between 256 and 512 MiB), so larger
+// filters are probed in passes of about 256 MiB each; filters up to 160 MiB
+// take one pass.  dtlg_set_probe_passes overrides the choice.
+uint32_t probe_passes(const dtlg_filter* f) {
+  const uint64_t bytes = (f->d.m_actual + 7) / 8;
+  uint64_t r = f->probe_passes;
+  if (r == 0) r = bytes <= (160ull << 20) ? 1 : std::max<uint64_t>(2, (bytes + (128ull << 20)) / (256ull << 20));
+  r = std::min<uint64_t>(r, 16);
+  r = std::min<uint64_t>(r, std::max<uint32_t>(1, f->d.addr.block_cnt));
+  return static_cast<uint32_t>(std::max<uint64_t>(1, r));
+}
+
 dtlg_status check_filter_ptr(const void* p) {
   if (!p) return DTLG_ERR_NULL;
   if (reinterpret_cast<uintptr_t>(p) & 15u) return DTLG_ERR_ALIGNMENT;
@@ -118,10 +155,10 @@ dtlg_status launch_probe(const dtlg_filter* f, const uint64_t* words, const uint
   }
   const uint32_t pre = static_cast<uint32_t>((reinterpret_cast<uintptr_t>(keys) & 15u) >> 2);
   const uint64_t n_phys = static_cast<uint64_t>(n) + pre;
-  const uint32_t tiles = probe_tiles(n_phys);
-  const size_t need = sizeof(WsHeader) + static_cast<size_t>(tiles) * 8;
-  if (ws_bytes < need) return DTLG_ERR_WORKSPACE;
-  DTLG_CUDA(cudaMemsetAsync(ws, 0, need, stream));
+  const bool two_pass = f->probe_mode == 2 || (f->probe_mode == 0 && n >= kTwoPassMinKeys);
+  const uint32_t tiles = two_pass ? compact_tiles(n_phys) : probe_tiles(n_phys);
+  if (ws_bytes < workspace_bytes(n_phys)) return DTLG_ERR_WORKSPACE;
+  DTLG_CUDA(cudaMemsetAsync(ws, 0, sizeof(WsHeader) + static_cast<size_t>(tiles) * 8, stream));
   WsHeader* h = static_cast<WsHeader*>(ws);
   ProbeArgs a{};
   a.filter = words;
@@ -137,11 +174,48 @@ dtlg_status launch_probe(const dtlg_filter* f, const uint64_t* words, const uint
   a.n_tiles = tiles;
   a.addr = f->d.addr;
   a.victim_word = f->d.victim_word;
-  const probe_fn fn = f->bk ? f->bk->probe : f->ck->probe;
-  const occ_fn occ = f->bk ? f->bk->probe_blocks_per_sm : f->ck->probe_blocks_per_sm;
-  const int per_sm = std::max(1, occ());
-  const int grid = static_cast<int>(std::min<uint64_t>(tiles, static_cast<uint64_t>(ds->sms) * per_sm));
-  DTLG_CUDA(fn(a, grid, stream));
+  if (!two_pass) {
+    const probe_fn fn = f->bk ? f->bk->probe : f->ck->probe;
+    const occ_fn occ = f->bk ? f->bk->probe_blocks_per_sm : f->ck->probe_blocks_per_sm;
+    const int per_sm = std::max(1, occ());
+    const int grid = static_cast<int>(std::min<uint64_t>(tiles, static_cast<uint64_t>(ds->sms) * per_sm));
+    DTLG_CUDA(fn(a, grid, stream));
+    return DTLG_OK;
+  }
+  // pass 1: match bitmask, in block-range passes over large filters (each pass
+  // probes only the keys whose block lies in its range, so the concurrently
+  // touched part of the filter stays within the GPU's address-translation reach)
+  uint32_t* bits = reinterpret_cast<uint32_t*>(reinterpret_cast<char*>(ws) + sizeof(WsHeader) + status_bytes(n_phys));
+  const int v = (f->bits_variant >= 0 && f->bits_variant < kBitsVariants) ? f->bits_variant : 1;
+  const probe_bits_fn bfn = f->bk ? f->bk->probe_bits[v] : f->ck->probe_bits[v];
+  const occ_fn bocc = f->bk ? f->bk->bits_blocks_per_sm[v] : f->ck->bits_blocks_per_sm[v];
+  const uint64_t chunks = (n_phys + 127) / 128;  // one warp-chunk = 128 keys
+  const uint64_t max_grid = static_cast<uint64_t>(ds->sms) * std::max(1, bocc());
+  const int bgrid = static_cast<int>(std::max<uint64_t>(1, std::min<uint64_t>((chunks + 7) / 8, max_grid)));
+  const uint32_t passes = probe_passes(f);
+  a.vec32 = (reinterpret_cast<uintptr_t>(words) & 31u) == 0 ? 1u : 0u;
+  const uint32_t nb = f->d.addr.block_cnt;
+  for (uint32_t r = 0; r < passes; r++) {
+    a.range_on = passes > 1 ? 1u : 0u;
+    a.blk_lo = static_cast<uint32_t>(static_cast<uint64_t>(nb) * r / passes);
+    a.blk_hi = r + 1 == passes ? 0xFFFFFFFFu : static_cast<uint32_t>(static_cast<uint64_t>(nb) * (r + 1) / passes);
+    DTLG_CUDA(bfn(a, bits, r > 0 ? 1 : 0, bgrid, stream));
+  }
+  // pass 2: ordered compaction
+  CompactArgs c{};
+  c.bits = bits;
+  c.n_words = bits_words(n_phys);
+  c.pre = pre;
+  c.match_offset = offset;
+  c.out = out;
+  c.count_out = count_dev;
+  c.status = a.status;
+  c.tile_ctr = a.tile_ctr;
+  c.err = a.err;
+  c.n_tiles = tiles;
+  const int cgrid = static_cast<int>(std::min<uint64_t>(tiles, static_cast<uint64_t>(ds->sms) * compact_occupancy()));
+  compact_kernel<<<cgrid, kCompactThreads, 0, stream>>>(c);
+  DTLG_CUDA(cudaGetLastError());
   return DTLG_OK;
 }
 
@@ -297,8 +371,36 @@ dtlg_status dtlg_batch_insert(const dtlg_filter* f, uint64_t* words, const uint3
   return DTLG_OK;
 }
 
-size_t dtlg_probe_workspace_size(uint32_t key_cnt) {
-  return sizeof(WsHeader) + static_cast<size_t>(probe_tiles(static_cast<uint64_t>(key_cnt) + 3)) * 8;
+size_t dtlg_probe_workspace_size(uint32_t key_cnt) { return workspace_bytes(static_cast<uint64_t>(key_cnt) + 3); }
+
+dtlg_status dtlg_set_l2_fetch_granularity(int bytes, int* in_effect) {
+  if (!(bytes == 0 || bytes == 32 || bytes == 64 || bytes == 128)) return DTLG_ERR_INVALID_CONFIG;
+  DTLG_CUDA(cudaDeviceSetLimit(cudaLimitMaxL2FetchGranularity, static_cast<size_t>(bytes)));
+  size_t v = 0;
+  DTLG_CUDA(cudaDeviceGetLimit(&v, cudaLimitMaxL2FetchGranularity));
+  if (in_effect) *in_effect = static_cast<int>(v);
+  return DTLG_OK;
+}
+
+int dtlg_probe_kernel_count(const dtlg_filter* f, uint32_t key_cnt) {
+  if (!f || key_cnt == 0) return 0;
+  const bool two_pass = f->probe_mode == 2 || (f->probe_mode == 0 && key_cnt >= kTwoPassMinKeys);
+  return two_pass ? static_cast<int>(probe_passes(f)) + 1 : 1;
+}
+
+dtlg_status dtlg_set_probe_passes(dtlg_filter* f, int passes) {
+  if (!f) return DTLG_ERR_NULL;
+  if (passes < 0 || passes > 16) return DTLG_ERR_INVALID_CONFIG;
+  f->probe_passes = passes;
+  return DTLG_OK;
+}
+
+dtlg_status dtlg_set_probe_options(dtlg_filter* f, int mode, int variant) {
+  if (!f) return DTLG_ERR_NULL;
+  if (mode < 0 || mode > 2 || variant < -1 || variant >= kBitsVariants) return DTLG_ERR_INVALID_CONFIG;
+  f->probe_mode = mode;
+  f->bits_variant = variant;
+  return DTLG_OK;
 }
 
 dtlg_status dtlg_batch_contains_ws(const dtlg_filter* f, const uint64_t* words, const uint32_t* keys,

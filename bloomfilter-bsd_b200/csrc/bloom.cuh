@@ -43,10 +43,30 @@ __device__ __forceinline__ void atomic_or_word(Word* p, Word m) {
   }
 }
 
-// Loads a whole block of W words with the widest aligned vector loads.
+// 256-bit load (sm_100): 32 bytes from a 32-byte aligned address.
+__device__ __forceinline__ void ld_nc_256(const void* p, unsigned long long& a, unsigned long long& b,
+                                          unsigned long long& c, unsigned long long& d) {
+  asm volatile("ld.global.nc.v4.u64 {%0,%1,%2,%3}, [%4];"
+               : "=l"(a), "=l"(b), "=l"(c), "=l"(d)
+               : "l"(p));
+}
+
+// Loads a whole block of W words with the widest aligned vector loads.  Each
+// load of a random block is one L1 wavefront, so fewer, wider loads raise the
+// probe rate: blocks of >= 32 bytes use 256-bit loads when the filter base is
+// 32-byte aligned (vec32), 128-bit loads otherwise.
 template <typename Word, int W>
-__device__ __forceinline__ void load_block(const Word* base, Word (&v)[W]) {
+__device__ __forceinline__ void load_block(const Word* base, Word (&v)[W], bool vec32 = false) {
   constexpr int kBytes = W * static_cast<int>(sizeof(Word));
+  if constexpr (kBytes >= 32) {
+    if (vec32) {
+      unsigned long long* d = reinterpret_cast<unsigned long long*>(&v[0]);
+      const unsigned long long* p = reinterpret_cast<const unsigned long long*>(base);
+#pragma unroll
+      for (int i = 0; i < kBytes / 32; i++) ld_nc_256(p + 4 * i, d[4 * i], d[4 * i + 1], d[4 * i + 2], d[4 * i + 3]);
+      return;
+    }
+  }
   if constexpr (kBytes >= 16) {
     const uint4* p = reinterpret_cast<const uint4*>(base);
 #pragma unroll
@@ -99,11 +119,13 @@ struct BloomOps {
   // Every bit of the key set?  ((word & mask) == mask over all touched words,
   // without early out, as blocked_bloomfilter.hpp:34 configures.)
   __device__ __forceinline__ static bool contains(const ProbeArgs& a, uint32_t key) {
-    const Word* base = block_ptr(a.filter, key, a.addr);
+    const uint32_t blk = block_index(key * mul_const(0), a.addr);
+    if (a.range_on && (blk < a.blk_lo || blk >= a.blk_hi)) return false;  // another pass's block
+    const Word* base = static_cast<const Word*>(a.filter) + static_cast<uint64_t>(blk) * kW;
     bool ok = true;
     if constexpr (kS.fixed_words) {
       Word v[kW];
-      load_block<Word, kW>(base, v);
+      load_block<Word, kW>(base, v, a.vec32 != 0);
       static_for<kS.ng>([&](auto G) {
         constexpr int g = decltype(G)::value;
         const Word m = group_mask<g>(key);

@@ -109,6 +109,13 @@ struct CuckooOps {
     const unsigned int* v = static_cast<const unsigned int*>(a.filter) + a.victim_word;
     const uint32_t vi = __ldg(v), vt = __ldg(v + 1), vu = __ldg(v + 2) & 0xffu;
     const bool in_victim = vu && tag == vt && (i1 == vi || i2 == vi);
+    if (a.range_on) {
+      // block-range pass: only the buckets this pass owns (the result is the OR
+      // over all passes)
+      const bool r1 = i1 >= a.blk_lo && i1 < a.blk_hi;
+      const bool r2 = i2 >= a.blk_lo && i2 < a.blk_hi;
+      return in_victim | (r1 && bucket_has(a.filter, i1, tag)) | (r2 && bucket_has(a.filter, i2, tag));
+    }
     return in_victim | bucket_has(a.filter, i1, tag) | bucket_has(a.filter, i2, tag);
   }
 

@@ -34,6 +34,12 @@ struct ProbeArgs {
   uint32_t n_tiles;
   Addr addr;
   uint64_t victim_word;         // cuckoo: 32-bit word index of the victim record
+  // Block-range pass (two-pass probe only; all zero = off): a key whose block
+  // (bucket) lies outside [blk_lo, blk_hi) is not probed in this pass.
+  uint32_t range_on, blk_lo, blk_hi;
+  // 1 when the filter base is 32-byte aligned: blocks of >= 32 bytes are then
+  // read with 256-bit loads.
+  uint32_t vec32;
 };
 
 constexpr int kProbeThreads = 256;

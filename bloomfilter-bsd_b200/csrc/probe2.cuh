@@ -1,0 +1,166 @@
+// probe2.cuh -- batch_contains as two streaming kernels, for large batches.
+//
+// 1. probe_bits_kernel: every warp takes chunks of 128 keys (one 16-byte key
+//    vector per lane), tests them, and writes the 128 match flags as four
+//    32-bit words of a key-ordered bitmask.  No barrier, no look-back: the only
+//    thing a warp ever waits for is its own filter loads.
+// 2. compact_kernel: turns the bitmask into the ascending position list.  A
+//    tile is 65536 keys (2048 mask words); the tile offset comes from a
+//    decoupled look-back (bounded waits, as in probe.cuh) over a few thousand
+//    status words.  It moves 1/8 byte per key in and 4 bytes per match out.
+// The extra traffic against the fused kernel is the bitmask, 2/8 byte per key.
+#pragma once
+
+#include <cstdint>
+
+#include "common.cuh"
+#include "probe.cuh"
+
+namespace dtlg {
+
+constexpr int kCompactThreads = 256;
+constexpr int kCompactWordsPerThread = 8;
+constexpr uint32_t kCompactTileWords = kCompactThreads * kCompactWordsPerThread;
+
+struct CompactArgs {
+  const uint32_t* bits;        // key-ordered match bitmask (bit i = physical key i)
+  uint64_t n_words;            // ceil(n_phys / 32)
+  uint32_t pre;                // physical index of the first key
+  uint32_t match_offset;
+  uint32_t* out;
+  unsigned long long* count_out;
+  unsigned long long* status;  // per-tile look-back words (zeroed)
+  unsigned int* tile_ctr;      // zeroed
+  unsigned int* err;           // zeroed
+  uint32_t n_tiles;
+};
+
+#ifdef __CUDACC__
+
+// or_into: a later block-range pass ORs its flags into the words of the
+// earlier passes (every word is written by exactly one warp per pass, and the
+// passes are ordered on one stream).
+template <class Ops, int MINB>
+__global__ void __launch_bounds__(256, MINB)
+probe_bits_kernel(const __grid_constant__ ProbeArgs a, uint32_t* __restrict__ bits, int or_into) {
+  const uint32_t lane = threadIdx.x & 31u;
+  const uint4* keys4 = reinterpret_cast<const uint4*>(a.keys_al);
+  const uint64_t n_vec = (a.n_phys + 3) >> 2;
+  const uint64_t n_words = (a.n_phys + 31) >> 5;
+  const uint64_t n_chunks = (n_vec + 31) >> 5;  // 32 key vectors = 128 keys
+  const uint64_t warps = static_cast<uint64_t>(gridDim.x) * (blockDim.x >> 5);
+  for (uint64_t c = static_cast<uint64_t>(blockIdx.x) * (blockDim.x >> 5) + (threadIdx.x >> 5); c < n_chunks;
+       c += warps) {
+    const uint64_t v = c * 32 + lane;
+    uint32_t f = 0;
+    if (v < n_vec) {
+      const uint4 kv = __ldcs(keys4 + v);
+      const uint32_t k[4] = {kv.x, kv.y, kv.z, kv.w};
+#pragma unroll
+      for (int q = 0; q < 4; q++) f |= (Ops::contains(a, k[q]) ? 1u : 0u) << q;
+      const uint64_t p0 = v * 4;
+      if (p0 < a.pre || p0 + 4 > a.n_phys) {
+#pragma unroll
+        for (int q = 0; q < 4; q++)
+          if (p0 + q < a.pre || p0 + q >= a.n_phys) f &= ~(1u << q);
+      }
+    }
+    // lanes 8j .. 8j+7 hold keys 32j .. 32j+31 of the chunk: word j
+    uint32_t x = f << (4u * (lane & 7u));
+    x |= __shfl_xor_sync(0xffffffffu, x, 1);
+    x |= __shfl_xor_sync(0xffffffffu, x, 2);
+    x |= __shfl_xor_sync(0xffffffffu, x, 4);
+    if ((lane & 7u) == 0) {
+      const uint64_t w = c * 4 + (lane >> 3);
+      if (w < n_words) {
+        if (or_into) x |= __ldcg(bits + w);
+        __stcg(bits + w, x);
+      }
+    }
+  }
+}
+
+static __global__ void __launch_bounds__(kCompactThreads) compact_kernel(const __grid_constant__ CompactArgs a) {
+  constexpr int kWarps = kCompactThreads / 32;
+  __shared__ uint32_t s_tile;
+  __shared__ uint32_t s_warp[kWarps];
+  __shared__ uint32_t s_excl;
+  const uint32_t lane = threadIdx.x & 31u;
+  const uint32_t warp = threadIdx.x >> 5;
+  // the look-back helper of probe.cuh reads status / err from a ProbeArgs
+  ProbeArgs lb{};
+  lb.status = a.status;
+  lb.err = a.err;
+  for (;;) {
+    if (threadIdx.x == 0) s_tile = atomicAdd(a.tile_ctr, 1u);
+    __syncthreads();
+    const uint32_t tile = s_tile;
+    if (tile >= a.n_tiles) break;
+    const uint64_t w0 = static_cast<uint64_t>(tile) * kCompactTileWords + threadIdx.x * kCompactWordsPerThread;
+    uint32_t wv[kCompactWordsPerThread];
+    if (w0 + kCompactWordsPerThread <= a.n_words) {
+      const uint4* p = reinterpret_cast<const uint4*>(a.bits + w0);
+      const uint4 x0 = __ldcs(p), x1 = __ldcs(p + 1);
+      wv[0] = x0.x; wv[1] = x0.y; wv[2] = x0.z; wv[3] = x0.w;
+      wv[4] = x1.x; wv[5] = x1.y; wv[6] = x1.z; wv[7] = x1.w;
+    } else {
+#pragma unroll
+      for (int i = 0; i < kCompactWordsPerThread; i++) wv[i] = (w0 + i < a.n_words) ? a.bits[w0 + i] : 0u;
+    }
+    uint32_t c = 0;
+#pragma unroll
+    for (int i = 0; i < kCompactWordsPerThread; i++) c += __popc(wv[i]);
+    uint32_t incl = c;
+#pragma unroll
+    for (int d = 1; d < 32; d <<= 1) {
+      const uint32_t t = __shfl_up_sync(0xffffffffu, incl, d);
+      if (lane >= static_cast<uint32_t>(d)) incl += t;
+    }
+    if (lane == 31) s_warp[warp] = incl;
+    __syncthreads();
+    if (warp == 0) {
+      const uint32_t v = lane < kWarps ? s_warp[lane] : 0u;
+      uint32_t wi = v;
+#pragma unroll
+      for (int d = 1; d < kWarps; d <<= 1) {
+        const uint32_t t = __shfl_up_sync(0xffffffffu, wi, d);
+        if (lane >= static_cast<uint32_t>(d)) wi += t;
+      }
+      const uint32_t agg = __shfl_sync(0xffffffffu, wi, kWarps - 1);
+      if (lane < kWarps) s_warp[lane] = wi - v;
+      uint32_t excl = 0;
+      if (tile == 0) {
+        if (lane == 0) st_volatile(a.status, kFlagPrefix | agg);
+      } else {
+        if (lane == 0) st_volatile(a.status + tile, kFlagAgg | agg);
+        excl = look_back(lb, tile, lane);
+        if (lane == 0) st_volatile(a.status + tile, kFlagPrefix | static_cast<uint32_t>(excl + agg));
+      }
+      if (lane == 0) {
+        s_excl = excl;
+        if (tile == a.n_tiles - 1) {
+          const bool failed = *reinterpret_cast<volatile unsigned int*>(a.err) != 0u;
+          *a.count_out = failed ? ~0ull : static_cast<unsigned long long>(excl) + agg;
+        }
+      }
+    }
+    __syncthreads();
+    uint32_t pos = s_excl + s_warp[warp] + (incl - c);
+    const uint32_t base = static_cast<uint32_t>(w0 * 32 - a.pre) + a.match_offset;
+#pragma unroll
+    for (int i = 0; i < kCompactWordsPerThread; i++) {
+      uint32_t m = wv[i];
+      while (m) {
+        const uint32_t b = __ffs(m) - 1;
+        m &= m - 1;
+        __stcs(a.out + pos, base + static_cast<uint32_t>(i) * 32u + b);
+        pos++;
+      }
+    }
+    __syncthreads();
+  }
+}
+
+#endif  // __CUDACC__
+
+}  // namespace dtlg

@@ -8,24 +8,34 @@
 #include "bloom.cuh"
 #include "cuckoo.cuh"
 #include "probe.cuh"
+#include "probe2.cuh"
 
 namespace dtlg {
 
 using probe_fn = cudaError_t (*)(const ProbeArgs&, int grid, cudaStream_t);
 using build_fn = cudaError_t (*)(const BuildArgs&, int grid, cudaStream_t);
 using occ_fn = int (*)();
+using probe_bits_fn = cudaError_t (*)(const ProbeArgs&, uint32_t* bits, int or_into, int grid, cudaStream_t);
+
+// Register-budget variants of probe_bits_kernel: 0 = 8 CTAs/SM (32 registers),
+// 1 = 4 CTAs/SM (64 registers, more filter loads in flight per thread).
+constexpr int kBitsVariants = 2;
 
 struct BloomKernels {
   uint32_t word_bytes, w, s, z, k;
   probe_fn probe;
   build_fn build;
   occ_fn probe_blocks_per_sm;
+  probe_bits_fn probe_bits[kBitsVariants];
+  occ_fn bits_blocks_per_sm[kBitsVariants];
 };
 
 struct CuckooKernels {
   uint32_t t, b;
   probe_fn probe;
   occ_fn probe_blocks_per_sm;
+  probe_bits_fn probe_bits[kBitsVariants];
+  occ_fn bits_blocks_per_sm[kBitsVariants];
   void (*unpack)(const uint32_t* table, uint32_t* slots, uint32_t buckets, int grid, cudaStream_t);
   void (*insert)(const CuckooBuildArgs&, int grid, cudaStream_t);
   void (*pack)(uint32_t* table, const uint32_t* slots, uint32_t buckets, uint64_t words, int grid,
@@ -45,6 +55,19 @@ constexpr int kProbeRounds = 4;
 constexpr uint32_t kProbeTile = kProbeThreads * 4 * kProbeRounds;
 
 #ifdef __CUDACC__
+template <class Ops, int MINB>
+struct BitsLaunch {
+  static cudaError_t run(const ProbeArgs& a, uint32_t* bits, int or_into, int grid, cudaStream_t s) {
+    probe_bits_kernel<Ops, MINB><<<grid, 256, 0, s>>>(a, bits, or_into);
+    return cudaGetLastError();
+  }
+  static int occupancy() {
+    int n = 0;
+    cudaOccupancyMaxActiveBlocksPerMultiprocessor(&n, probe_bits_kernel<Ops, MINB>, 256, 0);
+    return n;
+  }
+};
+
 template <class Cfg>
 struct BloomLaunch {
   static cudaError_t probe(const ProbeArgs& a, int grid, cudaStream_t s) {
@@ -66,8 +89,11 @@ struct BloomLaunch {
 template <typename Word, int W, int S, int Z, int K>
 BloomKernels bloom_entry() {
   using C = BloomCfg<Word, W, S, Z, K>;
+  using B8 = BitsLaunch<BloomOps<C>, 8>;
+  using B4 = BitsLaunch<BloomOps<C>, 4>;
   return BloomKernels{static_cast<uint32_t>(sizeof(Word)), W, S, Z, K, &BloomLaunch<C>::probe,
-                      &BloomLaunch<C>::build, &BloomLaunch<C>::occupancy};
+                      &BloomLaunch<C>::build, &BloomLaunch<C>::occupancy,
+                      {&B8::run, &B4::run}, {&B8::occupancy, &B4::occupancy}};
 }
 
 template <int T, int B>
@@ -101,7 +127,10 @@ struct CuckooLaunch {
 template <int T, int B>
 CuckooKernels cuckoo_entry() {
   using L = CuckooLaunch<T, B>;
-  return CuckooKernels{T, B, &L::probe, &L::occupancy, &L::unpack, &L::insert, &L::pack, &L::count};
+  using B8 = BitsLaunch<CuckooOps<CuckooCfg<T, B>>, 8>;
+  using B4 = BitsLaunch<CuckooOps<CuckooCfg<T, B>>, 4>;
+  return CuckooKernels{T, B, &L::probe, &L::occupancy, {&B8::run, &B4::run}, {&B8::occupancy, &B4::occupancy},
+                       &L::unpack, &L::insert, &L::pack, &L::count};
 }
 #endif
 

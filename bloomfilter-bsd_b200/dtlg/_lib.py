@@ -65,6 +65,10 @@ SIGNATURES = {
     "dtlg_probe_workspace_size": (C.c_size_t, [_u32]),
     "dtlg_batch_contains_ws": (_i, [_vp, _vp, _vp, _u32, _vp, _u32, _vp, _vp, C.c_size_t, _vp]),
     "dtlg_batch_contains_noalloc": (_i, [_vp, _vp, _vp, _u32, _vp, _u32, _vp, _vp]),
+    "dtlg_set_probe_options": (_i, [_vp, _i, _i]),
+    "dtlg_set_probe_passes": (_i, [_vp, _i]),
+    "dtlg_probe_kernel_count": (_i, [_vp, _u32]),
+    "dtlg_set_l2_fetch_granularity": (_i, [_i, C.POINTER(_i)]),
     "dtlg_insert": (_i, [_vp, _vp, _u32, _vp]),
     "dtlg_contains": (_i, [_vp, _vp, _u32, C.POINTER(_i), _vp]),
     "dtlg_batch_contains_host": (_i, [_vp, _vp, _vp, _u64, _vp, _u32, _u64p, _vp]),

@@ -115,6 +115,15 @@ class filter_base:  # noqa: N801 (reference name)
     def kind(self):
         return ("bloom", "zoned", "cuckoo")[lib().dtlg_kind(self._h)]
 
+    def set_probe_options(self, mode=0, variant=-1):
+        """Probe kernel choice (0 auto, 1 fused, 2 bitmask + compaction) and the
+        bitmask kernel's register budget; results are identical in all modes."""
+        check(lib().dtlg_set_probe_options(self._h, int(mode), int(variant)), "set_probe_options")
+
+    def set_probe_passes(self, passes=0):
+        """Block-range passes of the two-kernel probe (0 = automatic)."""
+        check(lib().dtlg_set_probe_passes(self._h, int(passes)), "set_probe_passes")
+
     def alloc_filter_data(self, device="cuda"):
         """Zeroed filter words, as the facade allocates them (filter.hpp:113-119)."""
         torch = _torch()
@@ -188,6 +197,14 @@ class filter_base:  # noqa: N801 (reference name)
             return False
         check(st, "batch_insert_host")
         return True
+
+
+def set_l2_fetch_granularity(nbytes):
+    """cudaLimitMaxL2FetchGranularity of the current device's context (this
+    process only); returns the value in effect."""
+    v = C.c_int(0)
+    check(lib().dtlg_set_l2_fetch_granularity(int(nbytes), C.byref(v)), "set_l2_fetch_granularity")
+    return v.value
 
 
 def _bloom_handle(m, k, word_size, w, s, z):

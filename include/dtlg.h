@@ -121,6 +121,29 @@ dtlg_status dtlg_batch_contains_ws(const dtlg_filter* f, const uint64_t* filter_
                                    uint32_t match_offset, uint64_t* match_cnt_dev, void* workspace,
                                    size_t workspace_bytes, dtlg_stream_t stream);
 
+/* Probe tuning of one filter (set by the autotuner, dtlg/autotune.py):
+ * mode 0 = automatic, 1 = one fused kernel (probe + ordered compaction),
+ * 2 = two streaming kernels (match bitmask, then compaction); variant selects
+ * the register budget of the bitmask kernel (-1 = automatic, 0 = 32 registers
+ * at 8 CTAs/SM, 1 = 64 registers at 4 CTAs/SM).  Results never change.
+ * (The reference's counterpart is its per-config SIMD unroll factor,
+ * blocked_bloomfilter_tune.hpp:21-56.) */
+dtlg_status dtlg_set_probe_options(dtlg_filter* f, int mode, int variant);
+/* Block-range passes of the two-kernel probe (0 = automatic, 1..16).  Random
+ * probes over more than ~256 MiB of filter exceed the GPU's address-translation
+ * reach; probing one block range per pass keeps each pass within it. */
+dtlg_status dtlg_set_probe_passes(dtlg_filter* f, int passes);
+/* Number of kernels one batch_contains of key_cnt keys launches with the
+ * current options (fused: 1; two-kernel: block-range passes + compaction). */
+int dtlg_probe_kernel_count(const dtlg_filter* f, uint32_t key_cnt);
+
+/* Sets the L2 fetch granularity hint of the CURRENT device's context
+ * (cudaLimitMaxL2FetchGranularity; 0, 32, 64 or 128 bytes) and returns the
+ * value in effect in *in_effect.  Random 32/64-byte filter reads waste HBM
+ * bandwidth when every miss fills a 128-byte line.  The limit belongs to this
+ * process's context only and ends with it. */
+dtlg_status dtlg_set_l2_fetch_granularity(int bytes, int* in_effect);
+
 /* ---- probe without any allocation (no counterpart in the reference) ----
  * For callers that cannot call cudaMalloc -- a query engine whose device
  * memory is all owned by its own buffer manager, a plugin inside a host

@@ -72,7 +72,10 @@ def test_bloom_every_config_bit_exact():
             pk, _ = keygen.probe_keys(n, 3001, 0.4, seed)
             off = (1 << 32) - 1500 if ci % 2 else 17
             exp = ob.batch_contains(ref_words, pk, off)
-            assert np.array_equal(gpu_probe(f, words, pk, off, pad=(ci + 1) % 4), exp), (wb, w, s, z, k, m)
+            for mode in (1, 2):  # fused kernel; bitmask + compaction (in 1-3 block-range passes)
+                f.set_probe_options(mode, ci % 2)
+                f.set_probe_passes(1 + ci % 3)
+                assert np.array_equal(gpu_probe(f, words, pk, off, pad=(ci + 1) % 4), exp), (wb, w, s, z, k, m, mode)
 
 
 def test_bloom_golden_vectors(golden):
@@ -98,8 +101,12 @@ def test_probe_lengths_and_alignment(n):
     ob.insert(rw, bk)
     words = dev_words(rw)
     pk, _ = keygen.probe_keys(20000, n, 0.5, 5)
-    for pad in range(4):
-        assert np.array_equal(gpu_probe(f, words, pk, 9, pad), ob.batch_contains(rw, pk, 9))
+    exp = ob.batch_contains(rw, pk, 9)
+    for mode, variant, passes in ((0, -1, 0), (1, -1, 0), (2, 0, 1), (2, 1, 1), (2, 1, 3), (2, 0, 16)):
+        f.set_probe_options(mode, variant)
+        f.set_probe_passes(passes)
+        for pad in range(4):
+            assert np.array_equal(gpu_probe(f, words, pk, 9, pad), exp), (mode, variant, passes, pad)
 
 
 def test_cuckoo_probe_every_config_bit_exact():
@@ -116,7 +123,10 @@ def test_cuckoo_probe_every_config_bit_exact():
             oc.insert(table, bk, seed=ci + 1)
             pk, _ = keygen.probe_keys(n, 5000, 0.3, 300 + ci)
             exp = oc.batch_contains(table, pk, 11)
-            assert np.array_equal(gpu_probe(f, dev_words(table), pk, 11, pad=ci % 4), exp), (t, b, m)
+            for mode, passes in ((1, 0), (2, 1), (2, 2), (2, 5)):
+                f.set_probe_options(mode, ci % 2)
+                f.set_probe_passes(passes)
+                assert np.array_equal(gpu_probe(f, dev_words(table), pk, 11, pad=ci % 4), exp), (t, b, m, mode, passes)
             assert f.count_occupied_slots(dev_words(table)) == oc.count_occupied(table)
 
 
