@@ -50,6 +50,9 @@ def parse():
     ap.add_argument("--workload", choices=sorted(WORKLOADS), default="sectorized_dram")
     ap.add_argument("--no-cpu-baseline", action="store_true")
     ap.add_argument("--no-e2e", action="store_true")
+    ap.add_argument("--probe-mode", type=int, default=0,
+                    help="0 auto, 1 fused, 2 bitmask + block-range passes, 3 partitioned")
+    ap.add_argument("--probe-passes", type=int, default=0, help="block-range passes of mode 2 (0 auto)")
     return ap.parse_args()
 
 
@@ -195,6 +198,8 @@ def run_dtlg(args):
     m = n_build * bpk
     cfg = dtlg.blocked_bloomfilter_config(k=k, word_size=wb, word_cnt_per_block=w, sector_cnt=s, zone_cnt=z)
     f = dtlg.construct(cfg, m)
+    f.set_probe_options(args.probe_mode, -1)
+    f.set_probe_passes(args.probe_passes)
     words = f.alloc_filter_data()
     bk = keygen.build_keys_torch(n_build, SEED)
     assert f.batch_insert(words, bk)

@@ -9,6 +9,7 @@
 #include "cuckoo.cuh"
 #include "probe.cuh"
 #include "probe2.cuh"
+#include "probe3.cuh"
 
 namespace dtlg {
 
@@ -20,6 +21,7 @@ using probe_bits_fn = cudaError_t (*)(const ProbeArgs&, uint32_t* bits, int or_i
 // Register-budget variants of probe_bits_kernel: 0 = 8 CTAs/SM (32 registers),
 // 1 = 4 CTAs/SM (64 registers, more filter loads in flight per thread).
 constexpr int kBitsVariants = 2;
+using pairs_fn = cudaError_t (*)(const PairsArgs&, int grid, cudaStream_t);
 
 struct BloomKernels {
   uint32_t word_bytes, w, s, z, k;
@@ -28,6 +30,8 @@ struct BloomKernels {
   occ_fn probe_blocks_per_sm;
   probe_bits_fn probe_bits[kBitsVariants];
   occ_fn bits_blocks_per_sm[kBitsVariants];
+  pairs_fn probe_pairs[kBitsVariants];
+  occ_fn pairs_blocks_per_sm[kBitsVariants];
 };
 
 struct CuckooKernels {
@@ -68,6 +72,19 @@ struct BitsLaunch {
   }
 };
 
+template <class Ops, int MINB>
+struct PairsLaunch {
+  static cudaError_t run(const PairsArgs& a, int grid, cudaStream_t s) {
+    probe_pairs_kernel<Ops, MINB><<<grid, 256, 0, s>>>(a);
+    return cudaGetLastError();
+  }
+  static int occupancy() {
+    int n = 0;
+    cudaOccupancyMaxActiveBlocksPerMultiprocessor(&n, probe_pairs_kernel<Ops, MINB>, 256, 0);
+    return n;
+  }
+};
+
 template <class Cfg>
 struct BloomLaunch {
   static cudaError_t probe(const ProbeArgs& a, int grid, cudaStream_t s) {
@@ -91,9 +108,12 @@ BloomKernels bloom_entry() {
   using C = BloomCfg<Word, W, S, Z, K>;
   using B8 = BitsLaunch<BloomOps<C>, 8>;
   using B4 = BitsLaunch<BloomOps<C>, 4>;
+  using P8 = PairsLaunch<BloomOps<C>, 8>;
+  using P4 = PairsLaunch<BloomOps<C>, 4>;
   return BloomKernels{static_cast<uint32_t>(sizeof(Word)), W, S, Z, K, &BloomLaunch<C>::probe,
                       &BloomLaunch<C>::build, &BloomLaunch<C>::occupancy,
-                      {&B8::run, &B4::run}, {&B8::occupancy, &B4::occupancy}};
+                      {&B8::run, &B4::run}, {&B8::occupancy, &B4::occupancy},
+                      {&P8::run, &P4::run}, {&P8::occupancy, &P4::occupancy}};
 }
 
 template <int T, int B>

@@ -72,7 +72,7 @@ def test_bloom_every_config_bit_exact():
             pk, _ = keygen.probe_keys(n, 3001, 0.4, seed)
             off = (1 << 32) - 1500 if ci % 2 else 17
             exp = ob.batch_contains(ref_words, pk, off)
-            for mode in (1, 2):  # fused kernel; bitmask + compaction (in 1-3 block-range passes)
+            for mode in (1, 2, 3):  # fused; bitmask (1-3 block-range passes); partitioned
                 f.set_probe_options(mode, ci % 2)
                 f.set_probe_passes(1 + ci % 3)
                 assert np.array_equal(gpu_probe(f, words, pk, off, pad=(ci + 1) % 4), exp), (wb, w, s, z, k, m, mode)
@@ -102,7 +102,8 @@ def test_probe_lengths_and_alignment(n):
     words = dev_words(rw)
     pk, _ = keygen.probe_keys(20000, n, 0.5, 5)
     exp = ob.batch_contains(rw, pk, 9)
-    for mode, variant, passes in ((0, -1, 0), (1, -1, 0), (2, 0, 1), (2, 1, 1), (2, 1, 3), (2, 0, 16)):
+    for mode, variant, passes in ((0, -1, 0), (1, -1, 0), (2, 0, 1), (2, 1, 1), (2, 1, 3), (2, 0, 16), (3, 0, 0),
+                                  (3, 1, 0)):
         f.set_probe_options(mode, variant)
         f.set_probe_passes(passes)
         for pad in range(4):
