@@ -47,7 +47,7 @@ def parse():
     ap.add_argument("--steps", type=int, default=100)
     ap.add_argument("--warmup", type=int, default=5)
     ap.add_argument("--impl", choices=("dtlg", "reference"), default="dtlg")
-    ap.add_argument("--workload", choices=sorted(WORKLOADS), default="sectorized_dram")
+    ap.add_argument("--workload", choices=sorted(WORKLOADS) + ["batched512"], default="sectorized_dram")
     ap.add_argument("--no-cpu-baseline", action="store_true")
     ap.add_argument("--no-e2e", action="store_true")
     ap.add_argument("--probe-mode", type=int, default=0,
@@ -415,10 +415,140 @@ def run_reference(args):
     }), flush=True)
 
 
+BATCH_CONFIGS = [(8, 8, 8, 2, 8), (8, 8, 8, 4, 8), (4, 16, 16, 2, 8), (4, 16, 16, 4, 8), (8, 8, 8, 1, 8)]
+
+
+def batched_plan(n_filters=512, seed=4242):
+    """512 filters: config from the zoned (2/4 zones, u64 w=8 and u32 w=16) and
+    sectorized (u64 w=8 s=8) set, n log-uniform over 2^10..2^24, probes
+    log-uniform over 2^12..2^24 at 5 % hits, 8/12/16 bits per key."""
+    import numpy as np
+    rng = np.random.default_rng(seed)
+    plan = []
+    for i in range(n_filters):
+        cfg = BATCH_CONFIGS[int(rng.integers(0, len(BATCH_CONFIGS)))]
+        n = int(2 ** rng.uniform(10, 24))
+        p = int(2 ** rng.uniform(12, 24))
+        bpk = int(rng.choice([8, 12, 16]))
+        plan.append((cfg, n * bpk, n, p))
+    return plan
+
+
+def run_batched(args):
+    """512 independent filters built and probed in one
+    persistent, graph-captured launch vs 512 separate per-filter calls."""
+    import ctypes as C
+
+    import torch
+
+    import dtlg
+    from dtlg import keygen
+    from dtlg.batch import Batch, BatchItem
+    torch.cuda.set_device(int(os.environ.get("LOCAL_RANK", "0")))
+    plan = batched_plan()
+    items = []
+    total_words = 0
+    filters = []
+    for (wb, w, s, z, k), m, n, p in plan:
+        f = dtlg.construct(dtlg.blocked_bloomfilter_config(k=k, word_size=wb, word_cnt_per_block=w, sector_cnt=s,
+                                                           zone_cnt=z), m)
+        filters.append(f)
+        total_words += (f.alloc_words() + 3) // 4 * 4  # keep every filter 32-byte aligned
+    # all filter words in one allocation, so that one memset resets them per step
+    arena = torch.zeros(total_words, dtype=torch.int64, device="cuda")
+    off = 0
+    n_build = n_probe = 0
+    for i, (f, (cfg, m, n, p)) in enumerate(zip(filters, plan)):
+        wds = arena[off:off + f.alloc_words()]
+        off += (f.alloc_words() + 3) // 4 * 4
+        bk = keygen.build_keys_torch(n, 7000 + i)
+        pk, _ = keygen.probe_keys_torch(n, p, 0.05, 7000 + i)
+        items.append(BatchItem(f, wds, bk, pk, torch.empty(p, dtype=torch.int32, device="cuda"),
+                               torch.zeros(1, dtype=torch.int64, device="cuda"), 0))
+        n_build += n
+        n_probe += p
+    stream = torch.cuda.current_stream()
+    L = dtlg.lib()
+    batch = Batch(items, use_graph=True)
+
+    def batched_step():
+        arena.zero_()
+        batch.run()
+
+    ws = [torch.empty(L.dtlg_probe_workspace_size(it.probe_keys.numel()), dtype=torch.uint8, device="cuda")
+          for it in items]
+
+    def per_filter_step():
+        arena.zero_()
+        for it, w in zip(items, ws):
+            st = L.dtlg_batch_insert(it.filter._h, C.c_void_p(it.filter_data.data_ptr()),
+                                     C.c_void_p(it.build_keys.data_ptr()), it.build_keys.numel(), None,
+                                     C.c_void_p(stream.cuda_stream))
+            assert st == 0, st
+            st = L.dtlg_batch_contains_ws(it.filter._h, C.c_void_p(it.filter_data.data_ptr()),
+                                          C.c_void_p(it.probe_keys.data_ptr()), it.probe_keys.numel(),
+                                          C.c_void_p(it.match_positions.data_ptr()), 0,
+                                          C.c_void_p(it.match_cnt.data_ptr()), C.c_void_p(w.data_ptr()),
+                                          w.numel(), C.c_void_p(stream.cuda_stream))
+            assert st == 0, st
+
+    def timed(fn, steps):
+        for _ in range(max(3, args.warmup)):
+            fn()
+        torch.cuda.synchronize()
+        a, b = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
+        a.record(stream)
+        for _ in range(steps):
+            fn()
+        b.record(stream)
+        torch.cuda.synchronize()
+        return a.elapsed_time(b) / steps
+
+    # results of the two paths must agree
+    per_filter_step()
+    torch.cuda.synchronize()
+    ref_counts = [int(it.match_cnt.item()) for it in items]
+    ref_sums = [int(it.match_positions[:c].to(torch.int64).sum().item()) for it, c in zip(items, ref_counts)]
+    batched_step()
+    torch.cuda.synchronize()
+    for it, c, sm in zip(items, ref_counts, ref_sums):
+        assert int(it.match_cnt.item()) == c
+        assert int(it.match_positions[:c].to(torch.int64).sum().item()) == sm
+    steps = max(3, min(args.steps, 20))
+    clocks = ClockSampler(int(os.environ.get("LOCAL_RANK", "0")))
+    clocks.start()
+    ms_batched = timed(batched_step, steps)
+    ms_per_filter = timed(per_filter_step, steps)
+    clk = clocks.stop()
+    per_filter_kernels = sum((1 if it.build_keys.numel() else 0) + L.dtlg_probe_kernel_count(it.filter._h,
+                                                                                           it.probe_keys.numel())
+                             for it in items)
+    result = {
+        "metric": "batched build+probe of 512 filters: probe Gkeys/s (one persistent graph launch)",
+        "value": round(n_probe / (ms_batched / 1e3) / 1e9, 3), "unit": "Gkeys/s", "n_gpus": 1, "steps": steps,
+        "warmup": max(3, args.warmup), "ms_per_step": round(ms_batched, 3), "higher_is_better": True,
+        "scaling": "weak", "vs_baseline": None, "dtype": "u32", "data": "synthetic: seeded u32 bijection keys",
+        "config": {"workload": "batched512", "filters": len(items), "build_keys_total": n_build,
+                   "probe_keys_total": n_probe, "hit_ratio": 0.05,
+                   "filter_configs": [f"u{c[0] * 8} w={c[1]} s={c[2]} z={c[3]} k={c[4]}" for c in BATCH_CONFIGS],
+                   "filter_bytes_total": total_words * 8,
+                   "step": "zero all filter words, build all filters, probe all filters"},
+        "per_filter": {"ms_per_step": round(ms_per_filter, 3), "kernels_per_step": per_filter_kernels + 1,
+                       "api": "dtlg_batch_insert + dtlg_batch_contains_ws per filter, one stream"},
+        "speedup_vs_per_filter": round(ms_per_filter / ms_batched, 3),
+        "gpu_launches": steps * (batch.kernel_count()),
+        "fallback_filters": batch.fallback_count(),
+        "clocks": clk,
+    }
+    print(json.dumps(result), flush=True)
+
+
 def main():
     args = parse()
     if args.impl == "reference":
         run_reference(args)
+    elif args.workload == "batched512":
+        run_batched(args)
     else:
         run_dtlg(args)
 

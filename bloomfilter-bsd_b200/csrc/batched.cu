@@ -1,0 +1,264 @@
+// batched.cu -- host side of the batched multi-filter build+probe (batched.cuh).
+//
+// No counterpart in the reference: there a query with many filters calls
+// filter_base::batch_insert and batch_contains once per filter
+// (filter_base.hpp:26,42-45).  dtlg_batch_prepare turns a list of such calls
+// into device tables once; dtlg_batch_run then executes all of them as one
+// persistent kernel, captured with its workspace reset into a CUDA graph.
+#include <cuda_runtime.h>
+
+#include <algorithm>
+#include <vector>
+
+#include "../../include/dtlg.h"
+#include "batched.cuh"
+#include "filter_handle.hpp"
+
+namespace {
+
+using namespace dtlg;
+
+// The configs compiled into the batched kernel: sectorized and zoned 64-byte
+// blocks (u64 w=8 s=8; u64 w=8 z=2/4; u32 w=16 z=2/4, all k=8) and
+// register-blocked u32 w=1 k=4/8.  Filters of any other config run as
+// separate launches inside the same graph.
+using Menu0 = BloomCfg<uint64_t, 8, 8, 1, 8>;
+using Menu1 = BloomCfg<uint64_t, 8, 8, 2, 8>;
+using Menu2 = BloomCfg<uint64_t, 8, 8, 4, 8>;
+using Menu3 = BloomCfg<uint32_t, 16, 16, 2, 8>;
+using Menu4 = BloomCfg<uint32_t, 16, 16, 4, 8>;
+using Menu5 = BloomCfg<uint32_t, 1, 1, 1, 4>;
+using Menu6 = BloomCfg<uint32_t, 1, 1, 1, 8>;
+struct MenuEntry {
+  uint32_t wb, w, s, z, k;
+};
+constexpr MenuEntry kMenu[] = {{8, 8, 8, 1, 8},   {8, 8, 8, 2, 8}, {8, 8, 8, 4, 8}, {4, 16, 16, 2, 8},
+                               {4, 16, 16, 4, 8}, {4, 1, 1, 1, 4}, {4, 1, 1, 1, 8}};
+constexpr auto kBatchedKernel = batched_kernel<Menu0, Menu1, Menu2, Menu3, Menu4, Menu5, Menu6>;
+
+int menu_index(const FilterDesc& d) {
+  for (int i = 0; i < static_cast<int>(sizeof(kMenu) / sizeof(kMenu[0])); i++) {
+    const MenuEntry& m = kMenu[i];
+    if (m.wb == d.word_bytes && m.w == d.w && m.s == d.s && m.z == d.z && m.k == d.k) return i;
+  }
+  return -1;
+}
+
+uint32_t tiles_of(uint32_t n) { return (n + kBatchTile - 1) / kBatchTile; }
+size_t round256(size_t b) { return (b + 255) / 256 * 256; }
+
+}  // namespace
+
+struct dtlg_batch {
+  std::vector<dtlg_batch_item> items;
+  std::vector<int> fallback;         // item indexes run as separate launches
+  std::vector<void*> fallback_ws;
+  std::vector<size_t> fallback_ws_bytes;
+  uint32_t n_menu = 0, n_build_tiles = 0, n_probe_tiles = 0;
+  BatchDesc* d_desc = nullptr;
+  uint32_t* d_build_map = nullptr;
+  uint32_t* d_probe_map = nullptr;
+  char* d_ctl = nullptr;             // ctl words | built counters | status words
+  size_t ctl_bytes = 0, built_off = 0, status_off = 0;
+  int sms = 0, occupancy = 1, ctas_per_sm = 0;
+  bool use_graph = false;
+  bool warm = false;
+  cudaGraphExec_t exec = nullptr;
+  cudaGraph_t graph = nullptr;
+  cudaStream_t cap = nullptr;
+};
+
+namespace {
+
+dtlg_status enqueue(dtlg_batch* b, cudaStream_t s) {
+  if (b->n_menu) {
+    if (cudaMemsetAsync(b->d_ctl, 0, b->ctl_bytes, s) != cudaSuccess) return DTLG_ERR_CUDA;
+    BatchArgs a{};
+    a.desc = b->d_desc;
+    a.n_filters = b->n_menu;
+    a.build_map = b->d_build_map;
+    a.probe_map = b->d_probe_map;
+    a.n_build_tiles = b->n_build_tiles;
+    a.n_probe_tiles = b->n_probe_tiles;
+    a.ctl = reinterpret_cast<unsigned int*>(b->d_ctl);
+    a.built = reinterpret_cast<unsigned int*>(b->d_ctl + b->built_off);
+    a.status = reinterpret_cast<unsigned long long*>(b->d_ctl + b->status_off);
+    const int per_sm = b->ctas_per_sm > 0 ? std::min(b->ctas_per_sm, b->occupancy) : b->occupancy;
+    const uint32_t work = std::max(b->n_build_tiles, b->n_probe_tiles);
+    const int grid = static_cast<int>(std::max<uint64_t>(1, std::min<uint64_t>(work, static_cast<uint64_t>(b->sms) * per_sm)));
+    kBatchedKernel<<<grid, kBatchThreads, 0, s>>>(a);
+    if (cudaGetLastError() != cudaSuccess) return DTLG_ERR_CUDA;
+  }
+  for (size_t j = 0; j < b->fallback.size(); j++) {
+    const dtlg_batch_item& it = b->items[b->fallback[j]];
+    dtlg_stream_t ds = reinterpret_cast<dtlg_stream_t>(s);
+    if (dtlg_status st = dtlg_batch_insert(it.filter, it.filter_words, it.build_keys, it.n_build, nullptr, ds)) return st;
+    if (dtlg_status st = dtlg_batch_contains_ws(it.filter, it.filter_words, it.probe_keys, it.n_probe,
+                                                it.match_positions, it.match_offset, it.match_cnt,
+                                                b->fallback_ws[j], b->fallback_ws_bytes[j], ds))
+      return st;
+  }
+  return DTLG_OK;
+}
+
+void release(dtlg_batch* b) {
+  if (b->exec) cudaGraphExecDestroy(b->exec);
+  if (b->graph) cudaGraphDestroy(b->graph);
+  if (b->cap) cudaStreamDestroy(b->cap);
+  cudaFree(b->d_desc);
+  cudaFree(b->d_build_map);
+  cudaFree(b->d_probe_map);
+  cudaFree(b->d_ctl);
+  for (void* p : b->fallback_ws) cudaFree(p);
+}
+
+}  // namespace
+
+extern "C" {
+
+dtlg_status dtlg_batch_prepare(const dtlg_batch_item* items, uint32_t n_items, int use_graph, dtlg_batch** out) {
+  if (!out || (n_items && !items)) return DTLG_ERR_NULL;
+  *out = nullptr;
+  dtlg_batch* b = new dtlg_batch();
+  b->items.assign(items, items + n_items);
+  b->use_graph = use_graph != 0;
+  std::vector<BatchDesc> desc;
+  std::vector<uint32_t> build_map, probe_map;
+  for (uint32_t i = 0; i < n_items; i++) {
+    const dtlg_batch_item& it = items[i];
+    if (!it.filter || !it.filter_words || !it.match_cnt || (it.n_build && !it.build_keys) ||
+        (it.n_probe && (!it.probe_keys || !it.match_positions))) {
+      delete b;
+      return DTLG_ERR_NULL;
+    }
+    if (it.filter->ck) {  // cuckoo builds synchronize; not part of a batch
+      delete b;
+      return DTLG_ERR_UNSUPPORTED;
+    }
+    const int mi = menu_index(it.filter->d);
+    const bool aligned = (reinterpret_cast<uintptr_t>(it.build_keys) & 15u) == 0 &&
+                         (reinterpret_cast<uintptr_t>(it.probe_keys) & 15u) == 0 &&
+                         (reinterpret_cast<uintptr_t>(it.filter_words) & 15u) == 0;
+    if (mi < 0 || !aligned) {
+      b->fallback.push_back(static_cast<int>(i));
+      continue;
+    }
+    BatchDesc d{};
+    d.addr = it.filter->d.addr;
+    d.cfg = static_cast<uint32_t>(mi);
+    d.words = it.filter_words;
+    d.build_keys = it.build_keys;
+    d.probe_keys = it.probe_keys;
+    d.out = it.match_positions;
+    d.count_out = reinterpret_cast<unsigned long long*>(it.match_cnt);
+    d.n_build = it.n_build;
+    d.n_probe = it.n_probe;
+    d.match_offset = it.match_offset;
+    d.build_tile0 = static_cast<uint32_t>(build_map.size());
+    d.n_build_tiles = tiles_of(it.n_build);
+    d.probe_tile0 = static_cast<uint32_t>(probe_map.size());
+    d.n_probe_tiles = tiles_of(it.n_probe);
+    const uint32_t f = static_cast<uint32_t>(desc.size());
+    build_map.insert(build_map.end(), d.n_build_tiles, f);
+    probe_map.insert(probe_map.end(), d.n_probe_tiles, f);
+    desc.push_back(d);
+  }
+  b->n_menu = static_cast<uint32_t>(desc.size());
+  b->n_build_tiles = static_cast<uint32_t>(build_map.size());
+  b->n_probe_tiles = static_cast<uint32_t>(probe_map.size());
+  int dev = 0;
+  bool ok = cudaGetDevice(&dev) == cudaSuccess &&
+            cudaDeviceGetAttribute(&b->sms, cudaDevAttrMultiProcessorCount, dev) == cudaSuccess &&
+            cudaOccupancyMaxActiveBlocksPerMultiprocessor(&b->occupancy, kBatchedKernel, kBatchThreads, 0) ==
+                cudaSuccess;
+  b->occupancy = std::max(1, b->occupancy);
+  b->built_off = 256;
+  b->status_off = b->built_off + round256(static_cast<size_t>(b->n_menu) * 4);
+  b->ctl_bytes = b->status_off + round256(static_cast<size_t>(b->n_probe_tiles) * 8);
+  if (ok && b->n_menu) {
+    ok = cudaMalloc(&b->d_desc, desc.size() * sizeof(BatchDesc)) == cudaSuccess &&
+         cudaMalloc(&b->d_build_map, std::max<size_t>(1, build_map.size()) * 4) == cudaSuccess &&
+         cudaMalloc(&b->d_probe_map, std::max<size_t>(1, probe_map.size()) * 4) == cudaSuccess &&
+         cudaMalloc(&b->d_ctl, b->ctl_bytes) == cudaSuccess &&
+         cudaMemcpy(b->d_desc, desc.data(), desc.size() * sizeof(BatchDesc), cudaMemcpyHostToDevice) == cudaSuccess &&
+         (build_map.empty() || cudaMemcpy(b->d_build_map, build_map.data(), build_map.size() * 4,
+                                          cudaMemcpyHostToDevice) == cudaSuccess) &&
+         (probe_map.empty() || cudaMemcpy(b->d_probe_map, probe_map.data(), probe_map.size() * 4,
+                                          cudaMemcpyHostToDevice) == cudaSuccess);
+  }
+  for (size_t j = 0; ok && j < b->fallback.size(); j++) {
+    const size_t wsb = dtlg_probe_workspace_size(items[b->fallback[j]].n_probe);
+    void* p = nullptr;
+    ok = cudaMalloc(&p, wsb) == cudaSuccess;
+    b->fallback_ws.push_back(p);
+    b->fallback_ws_bytes.push_back(wsb);
+  }
+  if (!ok) {
+    release(b);
+    delete b;
+    return DTLG_ERR_ALLOC;
+  }
+  *out = b;
+  return DTLG_OK;
+}
+
+dtlg_status dtlg_batch_set_ctas_per_sm(dtlg_batch* b, int ctas_per_sm) {
+  if (!b) return DTLG_ERR_NULL;
+  if (ctas_per_sm < 0) return DTLG_ERR_INVALID_CONFIG;
+  b->ctas_per_sm = ctas_per_sm;
+  if (b->exec) {  // the grid size is baked into the graph: capture again
+    cudaGraphExecDestroy(b->exec);
+    cudaGraphDestroy(b->graph);
+    b->exec = nullptr;
+    b->graph = nullptr;
+  }
+  return DTLG_OK;
+}
+
+dtlg_status dtlg_batch_run(dtlg_batch* b, dtlg_stream_t stream_) {
+  if (!b) return DTLG_ERR_NULL;
+  cudaStream_t stream = reinterpret_cast<cudaStream_t>(stream_);
+  if (!b->use_graph) return enqueue(b, stream);
+  if (!b->warm) {
+    // The first run goes straight to the stream: it loads every kernel it
+    // touches (module loading is not allowed while a stream is capturing).
+    // Later runs replay a graph captured from the second run.
+    b->warm = true;
+    return enqueue(b, stream);
+  }
+  if (!b->exec) {
+    if (!b->cap && cudaStreamCreateWithFlags(&b->cap, cudaStreamNonBlocking) != cudaSuccess) return DTLG_ERR_CUDA;
+    if (cudaStreamBeginCapture(b->cap, cudaStreamCaptureModeThreadLocal) != cudaSuccess) return DTLG_ERR_CUDA;
+    const dtlg_status st = enqueue(b, b->cap);
+    cudaGraph_t g = nullptr;
+    const cudaError_t e = cudaStreamEndCapture(b->cap, &g);
+    if (st != DTLG_OK) {
+      if (g) cudaGraphDestroy(g);
+      return st;
+    }
+    if (e != cudaSuccess) return DTLG_ERR_CUDA;
+    b->graph = g;
+    if (cudaGraphInstantiate(&b->exec, g, 0) != cudaSuccess) return DTLG_ERR_CUDA;
+  }
+  return cudaGraphLaunch(b->exec, stream) == cudaSuccess ? DTLG_OK : DTLG_ERR_CUDA;
+}
+
+int dtlg_batch_kernel_count(const dtlg_batch* b) {
+  if (!b) return 0;
+  int n = b->n_menu ? 1 : 0;
+  for (int i : b->fallback) {
+    const dtlg_batch_item& it = b->items[i];
+    n += (it.n_build ? 1 : 0) + dtlg_probe_kernel_count(it.filter, it.n_probe);
+  }
+  return n;
+}
+
+uint32_t dtlg_batch_fallback_count(const dtlg_batch* b) { return b ? static_cast<uint32_t>(b->fallback.size()) : 0; }
+
+void dtlg_batch_destroy(dtlg_batch* b) {
+  if (!b) return;
+  release(b);
+  delete b;
+}
+
+}  // extern "C"

@@ -51,13 +51,48 @@ __device__ __forceinline__ void ld_nc_256(const void* p, unsigned long long& a, 
                : "l"(p));
 }
 
+// Coherent (weak, L1-cacheable) loads for filter words written earlier in the
+// same kernel (the batched build+probe kernel); the .nc path above may only
+// read data that is constant for the whole kernel.
+__device__ __forceinline__ uint4 ld_weak_128(const void* p) {
+  uint4 r;
+  asm volatile("ld.global.v4.u32 {%0,%1,%2,%3}, [%4];" : "=r"(r.x), "=r"(r.y), "=r"(r.z), "=r"(r.w) : "l"(p));
+  return r;
+}
+__device__ __forceinline__ unsigned long long ld_weak_64(const void* p) {
+  unsigned long long r;
+  asm volatile("ld.global.u64 %0, [%1];" : "=l"(r) : "l"(p));
+  return r;
+}
+__device__ __forceinline__ unsigned int ld_weak_32(const void* p) {
+  unsigned int r;
+  asm volatile("ld.global.u32 %0, [%1];" : "=r"(r) : "l"(p));
+  return r;
+}
+
 // Loads a whole block of W words with the widest aligned vector loads.  Each
 // load of a random block is one L1 wavefront, so fewer, wider loads raise the
 // probe rate: blocks of >= 32 bytes use 256-bit loads when the filter base is
-// 32-byte aligned (vec32), 128-bit loads otherwise.
-template <typename Word, int W>
+// 32-byte aligned (vec32), 128-bit loads otherwise.  NC = false reads through
+// the coherent path (see ld_weak_128).
+template <typename Word, int W, bool NC = true>
 __device__ __forceinline__ void load_block(const Word* base, Word (&v)[W], bool vec32 = false) {
   constexpr int kBytes = W * static_cast<int>(sizeof(Word));
+  if constexpr (!NC) {
+    if constexpr (kBytes >= 16) {
+#pragma unroll
+      for (int i = 0; i < kBytes / 16; i++) {
+        const uint4 x = ld_weak_128(reinterpret_cast<const uint4*>(base) + i);
+        uint32_t* d = reinterpret_cast<uint32_t*>(&v[0]) + 4 * i;
+        d[0] = x.x; d[1] = x.y; d[2] = x.z; d[3] = x.w;
+      }
+    } else if constexpr (kBytes == 8) {
+      *reinterpret_cast<unsigned long long*>(&v[0]) = ld_weak_64(base);
+    } else {
+      v[0] = static_cast<Word>(ld_weak_32(base));
+    }
+    return;
+  }
   if constexpr (kBytes >= 32) {
     if (vec32) {
       unsigned long long* d = reinterpret_cast<unsigned long long*>(&v[0]);
@@ -121,11 +156,17 @@ struct BloomOps {
   __device__ __forceinline__ static bool contains(const ProbeArgs& a, uint32_t key) {
     const uint32_t blk = block_index(key * mul_const(0), a.addr);
     if (a.range_on && (blk < a.blk_lo || blk >= a.blk_hi)) return false;  // another pass's block
-    const Word* base = static_cast<const Word*>(a.filter) + static_cast<uint64_t>(blk) * kW;
+    return test_block<true>(static_cast<const Word*>(a.filter) + static_cast<uint64_t>(blk) * kW, key,
+                            a.vec32 != 0);
+  }
+
+  // The key's bits in the block at `base`; NC selects the read-only load path.
+  template <bool NC>
+  __device__ __forceinline__ static bool test_block(const Word* base, uint32_t key, bool vec32) {
     bool ok = true;
     if constexpr (kS.fixed_words) {
       Word v[kW];
-      load_block<Word, kW>(base, v, a.vec32 != 0);
+      load_block<Word, kW, NC>(base, v, vec32);
       static_for<kS.ng>([&](auto G) {
         constexpr int g = decltype(G)::value;
         const Word m = group_mask<g>(key);
@@ -135,11 +176,12 @@ struct BloomOps {
       static_for<kS.ng>([&](auto G) {
         constexpr int g = decltype(G)::value;
         const Word m = group_mask<g>(key);
+        const Word* p = base + group_word<g>(key);
         Word x;
         if constexpr (sizeof(Word) == 8) {
-          x = __ldg(reinterpret_cast<const unsigned long long*>(base) + group_word<g>(key));
+          x = NC ? __ldg(reinterpret_cast<const unsigned long long*>(p)) : ld_weak_64(p);
         } else {
-          x = __ldg(reinterpret_cast<const unsigned int*>(base) + group_word<g>(key));
+          x = NC ? __ldg(reinterpret_cast<const unsigned int*>(p)) : ld_weak_32(p);
         }
         ok &= (x & m) == m;
       });

@@ -45,6 +45,12 @@ class CuckooConfigS(C.Structure):
     _fields_ = [("bits_per_tag", C.c_uint32), ("tags_per_bucket", C.c_uint32), ("addr_mode", C.c_uint32)]
 
 
+class BatchItemS(C.Structure):
+    _fields_ = [("filter", C.c_void_p), ("filter_words", C.c_void_p), ("build_keys", C.c_void_p),
+                ("n_build", C.c_uint32), ("probe_keys", C.c_void_p), ("n_probe", C.c_uint32),
+                ("match_positions", C.c_void_p), ("match_offset", C.c_uint32), ("match_cnt", C.c_void_p)]
+
+
 # every entry point declared in include/dtlg.h: name -> (restype, argtypes)
 _vp, _u32, _u64, _i = C.c_void_p, C.c_uint32, C.c_uint64, C.c_int
 _u64p = C.POINTER(C.c_uint64)
@@ -69,6 +75,12 @@ SIGNATURES = {
     "dtlg_set_probe_passes": (_i, [_vp, _i]),
     "dtlg_probe_kernel_count": (_i, [_vp, _u32]),
     "dtlg_set_l2_fetch_granularity": (_i, [_i, C.POINTER(_i)]),
+    "dtlg_batch_prepare": (_i, [C.POINTER(BatchItemS), _u32, _i, C.POINTER(_vp)]),
+    "dtlg_batch_run": (_i, [_vp, _vp]),
+    "dtlg_batch_set_ctas_per_sm": (_i, [_vp, _i]),
+    "dtlg_batch_kernel_count": (_i, [_vp]),
+    "dtlg_batch_fallback_count": (_u32, [_vp]),
+    "dtlg_batch_destroy": (None, [_vp]),
     "dtlg_insert": (_i, [_vp, _vp, _u32, _vp]),
     "dtlg_contains": (_i, [_vp, _vp, _u32, C.POINTER(_i), _vp]),
     "dtlg_batch_contains_host": (_i, [_vp, _vp, _vp, _u64, _vp, _u32, _u64p, _vp]),

@@ -162,6 +162,39 @@ dtlg_status dtlg_batch_contains_noalloc(const dtlg_filter* f, const uint64_t* fi
                                         uint32_t* match_positions, uint32_t match_offset,
                                         uint64_t* match_cnt_dev, dtlg_stream_t stream);
 
+/* ---- many filters at once (no counterpart in the reference) ----
+ * A query with one filter per partition or semi-join calls batch_insert and
+ * batch_contains once per filter in the reference (filter_base.hpp:26,42-45).
+ * dtlg_batch_prepare turns such a list of calls into device tables (it
+ * allocates and copies; the buffers named by the items must stay valid and
+ * unchanged); dtlg_batch_run then builds and probes all filters in ONE
+ * persistent kernel (optionally replayed as a CUDA graph).  Results are those
+ * of the per-filter calls: each item's filter words after inserting its build
+ * keys, and its probe keys' ascending match positions + count (DEVICE).
+ * Bloom filters of the compiled menu (u64 w=8 s=8 k=8; zoned u64 w=8 and u32
+ * w=16 with z=2/4, k=8; u32 w=1 k=4/8) run inside the persistent kernel;
+ * other Bloom configs (or keys not 16-byte aligned) run as separate launches
+ * in the same stream / graph.  Cuckoo filters: DTLG_ERR_UNSUPPORTED. */
+typedef struct dtlg_batch_item {
+  const dtlg_filter* filter;
+  uint64_t* filter_words;        /* device, as for dtlg_batch_insert */
+  const uint32_t* build_keys;    /* device */
+  uint32_t n_build;
+  const uint32_t* probe_keys;    /* device */
+  uint32_t n_probe;
+  uint32_t* match_positions;     /* device, capacity >= n_probe */
+  uint32_t match_offset;
+  uint64_t* match_cnt;           /* device */
+} dtlg_batch_item;
+typedef struct dtlg_batch dtlg_batch;
+dtlg_status dtlg_batch_prepare(const dtlg_batch_item* items, uint32_t n_items, int use_graph, dtlg_batch** out);
+dtlg_status dtlg_batch_run(dtlg_batch* b, dtlg_stream_t stream);
+/* CTAs per SM of the persistent kernel (0 = as many as fit); set by the autotuner. */
+dtlg_status dtlg_batch_set_ctas_per_sm(dtlg_batch* b, int ctas_per_sm);
+int dtlg_batch_kernel_count(const dtlg_batch* b);
+uint32_t dtlg_batch_fallback_count(const dtlg_batch* b);
+void dtlg_batch_destroy(dtlg_batch* b);
+
 /* ---- single keys: filter_base::insert / contains (filter_base.hpp:22,32) ---- */
 dtlg_status dtlg_insert(const dtlg_filter* f, uint64_t* filter_words, uint32_t key, dtlg_stream_t stream);
 dtlg_status dtlg_contains(const dtlg_filter* f, const uint64_t* filter_words, uint32_t key,
