@@ -345,6 +345,8 @@ dtlg_status cuckoo_insert(const dtlg_filter* f, uint64_t* words, const uint32_t*
 }
 
 }  // namespace
+
+dtlg_status cuda_error_status(cudaError_t e) { return cuda_fail(e); }
 }  // namespace dtlg
 
 // =============================================================================

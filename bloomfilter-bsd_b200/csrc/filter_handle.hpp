@@ -3,6 +3,7 @@
 
 #include "host_config.hpp"
 #include "registry.hpp"
+#include "status.hpp"
 
 struct dtlg_filter {
   dtlg::FilterDesc d;

@@ -51,6 +51,17 @@ class BatchItemS(C.Structure):
                 ("match_positions", C.c_void_p), ("match_offset", C.c_uint32), ("match_cnt", C.c_void_p)]
 
 
+class CostTablesS(C.Structure):
+    _fields_ = [("n_cand", C.c_uint32), ("n_bpk", C.c_uint32), ("bits_per_key", C.c_void_p), ("fpr", C.c_void_p),
+                ("n_size", C.c_uint32), ("log2_bytes_first", C.c_double), ("log2_bytes_step", C.c_double),
+                ("ns_per_key", C.c_void_p), ("ns_per_match", C.c_double), ("l2_budget_bytes", C.c_double)]
+
+
+class CostQueryS(C.Structure):
+    _fields_ = [("log2_n", C.c_double), ("fpr_target", C.c_double), ("hit_ratio", C.c_double),
+                ("work_ns", C.c_double), ("l2_resident", C.c_uint32)]
+
+
 # every entry point declared in include/dtlg.h: name -> (restype, argtypes)
 _vp, _u32, _u64, _i = C.c_void_p, C.c_uint32, C.c_uint64, C.c_int
 _u64p = C.POINTER(C.c_uint64)
@@ -81,6 +92,19 @@ SIGNATURES = {
     "dtlg_batch_kernel_count": (_i, [_vp]),
     "dtlg_batch_fallback_count": (_u32, [_vp]),
     "dtlg_batch_destroy": (None, [_vp]),
+    "dtlg_cost_search": (_i, [C.POINTER(CostTablesS), _vp, _u32, _vp, _vp, _vp, _vp, _vp, _i]),
+    "dtlg_cost_eval": (_i, [C.POINTER(CostTablesS), _vp, _u32, _vp, _vp, _vp]),
+    "dtlg_mlp_create": (_i, [_u32, _u32, _u32, _u32, _u32, C.POINTER(_vp)]),
+    "dtlg_mlp_destroy": (None, [_vp]),
+    "dtlg_mlp_param_count": (_u64, [_vp]),
+    "dtlg_mlp_set_params": (_i, [_vp, _vp]),
+    "dtlg_mlp_get_params": (_i, [_vp, _vp]),
+    "dtlg_mlp_get_grads": (_i, [_vp, _vp]),
+    "dtlg_mlp_forward": (_i, [_vp, _vp, _u32, _vp, _vp]),
+    "dtlg_mlp_loss_grad": (_i, [_vp, _vp, _vp, _vp, _u32, _vp, _vp]),
+    "dtlg_mlp_adam_step": (_i, [_vp, C.c_float, C.c_float, C.c_float, C.c_float, _vp]),
+    "dtlg_mlp_train": (_i, [_vp, _vp, _vp, _vp, _u32, _vp, _u32, _u32, C.c_float, C.c_float, _vp, _vp]),
+    "dtlg_mlp_choose": (_i, [_vp, _vp, _u32, _u32, _vp, _vp, _vp, _vp]),
     "dtlg_insert": (_i, [_vp, _vp, _u32, _vp]),
     "dtlg_contains": (_i, [_vp, _vp, _u32, C.POINTER(_i), _vp]),
     "dtlg_batch_contains_host": (_i, [_vp, _vp, _vp, _u64, _vp, _u32, _u64p, _vp]),

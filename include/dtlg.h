@@ -195,6 +195,74 @@ int dtlg_batch_kernel_count(const dtlg_batch* b);
 uint32_t dtlg_batch_fallback_count(const dtlg_batch* b);
 void dtlg_batch_destroy(dtlg_batch* b);
 
+/* ---- configuration choice: exhaustive calibrated search and MLP cost model ----
+ * Replaces the reference's model/ directory: cost_fn::overhead
+ * (model/cost_fn.hpp:150-160) minimised over m by model::optimizer
+ * (model/optimizer.hpp:25-140) for every configuration, as
+ * build_skyline_matrix does (tool/calibration/src/skyline_matrix_builder.cpp:
+ * 88-115).  Host memory throughout; the lookup times come from GPU calibration
+ * runs (t per key at log2-spaced filter sizes).
+ *   cost(c, bpk) = t_c(n * bpk / 8 bytes) + ns_per_match * (h + (1 - h) f)
+ *                  + work_ns * (1 - h) f,    f = fpr_c(bpk) <= fpr_target */
+typedef struct dtlg_cost_tables {
+  uint32_t n_cand;              /* C candidate configurations */
+  uint32_t n_bpk;               /* K bits-per-key grid points */
+  const double* bits_per_key;   /* [K], ascending */
+  const double* fpr;            /* [C*K]; +inf where the layout cannot hold the keys */
+  uint32_t n_size;              /* S calibrated filter sizes */
+  double log2_bytes_first;      /* size i is 2^(first + i * step) bytes */
+  double log2_bytes_step;
+  const double* ns_per_key;     /* [C*S] probe time per key */
+  double ns_per_match;          /* added time per matching key */
+  double l2_budget_bytes;       /* size limit of l2_resident queries */
+} dtlg_cost_tables;
+typedef struct dtlg_cost_query {
+  double log2_n;                /* build keys */
+  double fpr_target;            /* the filter's FPR must not exceed it */
+  double hit_ratio;             /* share of probe keys in the build set */
+  double work_ns;               /* downstream work per tuple that passes the filter */
+  uint32_t l2_resident;         /* 1: the filter must fit l2_budget_bytes */
+} dtlg_cost_query;
+/* Every candidate's least cost over the grid (cand_cost / cand_bpk [Q*C], may
+ * be NULL; +inf / NaN when infeasible) and the best candidate (best = -1 when
+ * none is feasible).  threads <= 0: all host cores. */
+dtlg_status dtlg_cost_search(const dtlg_cost_tables* t, const dtlg_cost_query* queries, uint32_t n_queries,
+                             double* cand_cost, double* cand_bpk, int32_t* best, double* best_cost,
+                             double* best_bpk, int threads);
+/* The cost of given choices (candidate, bits-per-key grid index); +inf if infeasible. */
+dtlg_status dtlg_cost_eval(const dtlg_cost_tables* t, const dtlg_cost_query* queries, uint32_t n_queries,
+                           const int32_t* cand, const uint32_t* bpk_index, double* cost);
+
+/* The MLP cost model: `hidden_layers` ReLU layers of `width` FP32 units and a
+ * linear output layer, trained and evaluated by this library's own kernels on
+ * the current device (forward, backward, Adam).  Parameters: for each layer
+ * W [in x out] row-major then b [out], back to back.  Device pointers for
+ * x / t / w / y / batch_rows / loss; host pointers for get/set_params.
+ * Loss = (1/N) sum w_ij (y_ij - t_ij)^2.  No counterpart in the reference. */
+typedef struct dtlg_mlp dtlg_mlp;
+dtlg_status dtlg_mlp_create(uint32_t n_in, uint32_t width, uint32_t hidden_layers, uint32_t n_out,
+                            uint32_t max_batch, dtlg_mlp** out);
+void dtlg_mlp_destroy(dtlg_mlp* m);
+uint64_t dtlg_mlp_param_count(const dtlg_mlp* m);
+dtlg_status dtlg_mlp_set_params(dtlg_mlp* m, const float* params_host);  /* also resets Adam state */
+dtlg_status dtlg_mlp_get_params(const dtlg_mlp* m, float* params_host);
+dtlg_status dtlg_mlp_get_grads(const dtlg_mlp* m, float* grads_host);
+dtlg_status dtlg_mlp_forward(dtlg_mlp* m, const float* x, uint32_t n, float* y, dtlg_stream_t stream);
+/* Loss and gradients of one batch of n <= max_batch rows; *loss (device) = L. */
+dtlg_status dtlg_mlp_loss_grad(dtlg_mlp* m, const float* x, const float* t, const float* w, uint32_t n,
+                               float* loss, dtlg_stream_t stream);
+dtlg_status dtlg_mlp_adam_step(dtlg_mlp* m, float lr, float beta1, float beta2, float eps, dtlg_stream_t stream);
+/* `steps` Adam steps (beta 0.9 / 0.999, eps 1e-8, cosine learning-rate decay
+ * lr_start -> lr_end) on batches of `batch` rows: step s uses rows
+ * batch_rows[s*batch .. s*batch+batch-1] of (x, t, w); loss_curve[s] = its loss. */
+dtlg_status dtlg_mlp_train(dtlg_mlp* m, const float* x, const float* t, const float* w, uint32_t n_rows,
+                           const uint32_t* batch_rows, uint32_t batch, uint32_t steps, float lr_start,
+                           float lr_end, float* loss_curve, dtlg_stream_t stream);
+/* Forward (into y_scratch [n x n_out]) and per row the argmin of the first
+ * n_cand outputs (choice) and output n_cand + choice (aux, may be NULL). */
+dtlg_status dtlg_mlp_choose(dtlg_mlp* m, const float* x, uint32_t n, uint32_t n_cand, float* y_scratch,
+                            int32_t* choice, float* aux, dtlg_stream_t stream);
+
 /* ---- single keys: filter_base::insert / contains (filter_base.hpp:22,32) ---- */
 dtlg_status dtlg_insert(const dtlg_filter* f, uint64_t* filter_words, uint32_t key, dtlg_stream_t stream);
 dtlg_status dtlg_contains(const dtlg_filter* f, const uint64_t* filter_words, uint32_t key,
