@@ -51,6 +51,12 @@ size_t round256(size_t b) { return (b + 255) / 256 * 256; }
 
 struct dtlg_batch {
   std::vector<dtlg_batch_item> items;
+  std::vector<BatchDesc> desc;       // host copy (with staging as planned at prepare)
+  uint32_t* d_bucket = nullptr;      // all staged filters' range buckets
+  uint2* d_range_items = nullptr;
+  uint32_t n_range_items = 0;
+  size_t ranges_built_off = 0, cursor_off = 0;
+  int staging = 0;                   // 0: stage every filter that fits, 1: never
   std::vector<int> fallback;         // item indexes run as separate launches
   std::vector<void*> fallback_ws;
   std::vector<size_t> fallback_ws_bytes;
@@ -82,11 +88,14 @@ dtlg_status enqueue(dtlg_batch* b, cudaStream_t s) {
     a.n_probe_tiles = b->n_probe_tiles;
     a.ctl = reinterpret_cast<unsigned int*>(b->d_ctl);
     a.built = reinterpret_cast<unsigned int*>(b->d_ctl + b->built_off);
+    a.ranges_built = reinterpret_cast<unsigned int*>(b->d_ctl + b->ranges_built_off);
+    a.range_items = b->d_range_items;
+    a.n_range_items = b->staging == 1 ? 0u : b->n_range_items;
     a.status = reinterpret_cast<unsigned long long*>(b->d_ctl + b->status_off);
     const int per_sm = b->ctas_per_sm > 0 ? std::min(b->ctas_per_sm, b->occupancy) : b->occupancy;
     const uint32_t work = std::max(b->n_build_tiles, b->n_probe_tiles);
     const int grid = static_cast<int>(std::max<uint64_t>(1, std::min<uint64_t>(work, static_cast<uint64_t>(b->sms) * per_sm)));
-    kBatchedKernel<<<grid, kBatchThreads, 0, s>>>(a);
+    kBatchedKernel<<<grid, kBatchThreads, kBatchRangeBytes, s>>>(a);
     if (cudaGetLastError() != cudaSuccess) return DTLG_ERR_CUDA;
   }
   for (size_t j = 0; j < b->fallback.size(); j++) {
@@ -109,7 +118,20 @@ void release(dtlg_batch* b) {
   cudaFree(b->d_build_map);
   cudaFree(b->d_probe_map);
   cudaFree(b->d_ctl);
+  cudaFree(b->d_bucket);
+  cudaFree(b->d_range_items);
   for (void* p : b->fallback_ws) cudaFree(p);
+}
+
+uint32_t log2_u32(uint32_t v) { return 31u - static_cast<uint32_t>(__builtin_clz(v)); }
+
+// Uploads the descriptor table, every filter staged as planned unless staging is off.
+bool upload_desc(dtlg_batch* b) {
+  std::vector<BatchDesc> d = b->desc;
+  for (size_t f = 0; f < d.size(); f++)
+    if (b->staging == 1) d[f].staged = 0;
+  return d.empty() ||
+         cudaMemcpy(b->d_desc, d.data(), d.size() * sizeof(BatchDesc), cudaMemcpyHostToDevice) == cudaSuccess;
 }
 
 }  // namespace
@@ -163,24 +185,60 @@ dtlg_status dtlg_batch_prepare(const dtlg_batch_item* items, uint32_t n_items, i
     probe_map.insert(probe_map.end(), d.n_probe_tiles, f);
     desc.push_back(d);
   }
+  // Staged build: ranges of kBatchRangeBytes; buckets with 25 % + 64 keys of
+  // slack over the expected share (overflow takes the direct path).
+  std::vector<uint2> range_items;
+  size_t bucket_words = 0, cursor_words = 0;
+  std::vector<size_t> bucket_at(desc.size()), cursor_at(desc.size());
+  for (size_t f = 0; f < desc.size(); f++) {
+    BatchDesc& d = desc[f];
+    const uint32_t block_bytes = kMenu[d.cfg].wb * kMenu[d.cfg].w;
+    const uint32_t bpr = kBatchRangeBytes / block_bytes;  // blocks per range (a power of two)
+    const uint32_t n_ranges = (d.addr.block_cnt + bpr - 1) / bpr;
+    if (d.n_build == 0 || n_ranges > kBatchMaxRanges) continue;
+    d.staged = 1;
+    d.n_ranges = n_ranges;
+    d.range_shift = log2_u32(bpr);
+    d.bucket_cap = static_cast<uint32_t>((static_cast<uint64_t>(d.n_build) * 5 / 4 + n_ranges - 1) / n_ranges) + 64;
+    bucket_at[f] = bucket_words;
+    cursor_at[f] = cursor_words;
+    bucket_words += static_cast<size_t>(n_ranges) * d.bucket_cap;
+    cursor_words += n_ranges;
+    for (uint32_t r = 0; r < n_ranges; r++) range_items.push_back(make_uint2(static_cast<uint32_t>(f), r));
+  }
+  b->n_range_items = static_cast<uint32_t>(range_items.size());
   b->n_menu = static_cast<uint32_t>(desc.size());
   b->n_build_tiles = static_cast<uint32_t>(build_map.size());
   b->n_probe_tiles = static_cast<uint32_t>(probe_map.size());
   int dev = 0;
   bool ok = cudaGetDevice(&dev) == cudaSuccess &&
             cudaDeviceGetAttribute(&b->sms, cudaDevAttrMultiProcessorCount, dev) == cudaSuccess &&
-            cudaOccupancyMaxActiveBlocksPerMultiprocessor(&b->occupancy, kBatchedKernel, kBatchThreads, 0) ==
-                cudaSuccess;
+            cudaOccupancyMaxActiveBlocksPerMultiprocessor(&b->occupancy, kBatchedKernel, kBatchThreads,
+                                                          kBatchRangeBytes) == cudaSuccess;
   b->occupancy = std::max(1, b->occupancy);
   b->built_off = 256;
-  b->status_off = b->built_off + round256(static_cast<size_t>(b->n_menu) * 4);
+  b->ranges_built_off = b->built_off + round256(static_cast<size_t>(b->n_menu) * 4);
+  b->cursor_off = b->ranges_built_off + round256(static_cast<size_t>(b->n_menu) * 4);
+  b->status_off = b->cursor_off + round256(cursor_words * 4);
   b->ctl_bytes = b->status_off + round256(static_cast<size_t>(b->n_probe_tiles) * 8);
+  if (ok && b->n_menu) {
+    ok = cudaMalloc(&b->d_ctl, b->ctl_bytes) == cudaSuccess &&
+         cudaMalloc(&b->d_bucket, std::max<size_t>(1, bucket_words) * 4) == cudaSuccess &&
+         cudaMalloc(&b->d_range_items, std::max<size_t>(1, range_items.size()) * sizeof(uint2)) == cudaSuccess &&
+         (range_items.empty() || cudaMemcpy(b->d_range_items, range_items.data(), range_items.size() * sizeof(uint2),
+                                            cudaMemcpyHostToDevice) == cudaSuccess);
+    for (size_t f = 0; ok && f < desc.size(); f++) {
+      if (!desc[f].staged) continue;
+      desc[f].bucket = b->d_bucket + bucket_at[f];
+      desc[f].cursor = reinterpret_cast<unsigned int*>(b->d_ctl + b->cursor_off) + cursor_at[f];
+    }
+    b->desc = desc;
+  }
   if (ok && b->n_menu) {
     ok = cudaMalloc(&b->d_desc, desc.size() * sizeof(BatchDesc)) == cudaSuccess &&
          cudaMalloc(&b->d_build_map, std::max<size_t>(1, build_map.size()) * 4) == cudaSuccess &&
          cudaMalloc(&b->d_probe_map, std::max<size_t>(1, probe_map.size()) * 4) == cudaSuccess &&
-         cudaMalloc(&b->d_ctl, b->ctl_bytes) == cudaSuccess &&
-         cudaMemcpy(b->d_desc, desc.data(), desc.size() * sizeof(BatchDesc), cudaMemcpyHostToDevice) == cudaSuccess &&
+         upload_desc(b) &&
          (build_map.empty() || cudaMemcpy(b->d_build_map, build_map.data(), build_map.size() * 4,
                                           cudaMemcpyHostToDevice) == cudaSuccess) &&
          (probe_map.empty() || cudaMemcpy(b->d_probe_map, probe_map.data(), probe_map.size() * 4,
@@ -241,6 +299,69 @@ dtlg_status dtlg_batch_run(dtlg_batch* b, dtlg_stream_t stream_) {
     if (cudaGraphInstantiate(&b->exec, g, 0) != cudaSuccess) return DTLG_ERR_CUDA;
   }
   return cudaGraphLaunch(b->exec, stream) == cudaSuccess ? DTLG_OK : DTLG_ERR_CUDA;
+}
+
+dtlg_status dtlg_batch_set_staging(dtlg_batch* b, int staging) {
+  if (!b) return DTLG_ERR_NULL;
+  if (staging < 0 || staging > 1) return DTLG_ERR_INVALID_CONFIG;
+  if (staging == b->staging) return DTLG_OK;
+  b->staging = staging;
+  if (b->n_menu && !upload_desc(b)) return DTLG_ERR_CUDA;
+  if (b->exec) {  // the range-queue length is baked into the graph: capture again
+    cudaGraphExecDestroy(b->exec);
+    cudaGraphDestroy(b->graph);
+    b->exec = nullptr;
+    b->graph = nullptr;
+  }
+  return DTLG_OK;
+}
+
+dtlg_status dtlg_batch_autotune(dtlg_batch* b, int reps, dtlg_stream_t stream_, dtlg_batch_plan* best_out) {
+  if (!b) return DTLG_ERR_NULL;
+  cudaStream_t stream = reinterpret_cast<cudaStream_t>(stream_);
+  reps = std::max(1, std::min(reps, 20));
+  std::vector<int> ctas = {0};
+  for (int c : {2, 3, 4, 6})
+    if (c < b->occupancy) ctas.push_back(c);
+  cudaEvent_t e0 = nullptr, e1 = nullptr;
+  cudaEventCreate(&e0);
+  cudaEventCreate(&e1);
+  dtlg_status st = DTLG_OK;
+  dtlg_batch_plan best{b->staging, b->ctas_per_sm, 0.f};
+  for (int sg : {0, 1}) {
+    for (int c : ctas) {
+      if ((st = dtlg_batch_set_staging(b, sg)) || (st = dtlg_batch_set_ctas_per_sm(b, c))) break;
+      for (int w = 0; w < 2 && st == DTLG_OK; w++) st = dtlg_batch_run(b, stream_);  // warm + capture
+      std::vector<float> ms;
+      for (int r = 0; r < reps && st == DTLG_OK; r++) {
+        cudaEventRecord(e0, stream);
+        st = dtlg_batch_run(b, stream_);
+        cudaEventRecord(e1, stream);
+        float t = 0.f;
+        if (cudaEventSynchronize(e1) != cudaSuccess || cudaEventElapsedTime(&t, e0, e1) != cudaSuccess)
+          st = DTLG_ERR_CUDA;
+        ms.push_back(t);
+      }
+      if (st != DTLG_OK) break;
+      std::sort(ms.begin(), ms.end());
+      if (best.ms == 0.f || ms[ms.size() / 2] < best.ms) best = {sg, c, ms[ms.size() / 2]};
+    }
+    if (st != DTLG_OK) break;
+  }
+  cudaEventDestroy(e0);
+  cudaEventDestroy(e1);
+  if (st != DTLG_OK) return st;
+  if ((st = dtlg_batch_set_staging(b, best.staging)) || (st = dtlg_batch_set_ctas_per_sm(b, best.ctas_per_sm)))
+    return st;
+  if (best_out) *best_out = best;
+  return DTLG_OK;
+}
+
+uint32_t dtlg_batch_staged_count(const dtlg_batch* b) {
+  if (!b || b->staging == 1) return 0;
+  uint32_t n = 0;
+  for (const BatchDesc& d : b->desc) n += d.staged ? 1u : 0u;
+  return n;
 }
 
 int dtlg_batch_kernel_count(const dtlg_batch* b) {

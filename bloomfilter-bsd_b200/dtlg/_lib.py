@@ -51,6 +51,15 @@ class BatchItemS(C.Structure):
                 ("match_positions", C.c_void_p), ("match_offset", C.c_uint32), ("match_cnt", C.c_void_p)]
 
 
+class ProbePlanS(C.Structure):
+    _fields_ = [("mode", C.c_int), ("variant", C.c_int), ("passes", C.c_int), ("ms", C.c_float),
+                ("gkeys_per_s", C.c_float)]
+
+
+class BatchPlanS(C.Structure):
+    _fields_ = [("staging", C.c_int), ("ctas_per_sm", C.c_int), ("ms", C.c_float)]
+
+
 class CostTablesS(C.Structure):
     _fields_ = [("n_cand", C.c_uint32), ("n_bpk", C.c_uint32), ("bits_per_key", C.c_void_p), ("fpr", C.c_void_p),
                 ("n_size", C.c_uint32), ("log2_bytes_first", C.c_double), ("log2_bytes_step", C.c_double),
@@ -86,6 +95,10 @@ SIGNATURES = {
     "dtlg_set_probe_passes": (_i, [_vp, _i]),
     "dtlg_probe_kernel_count": (_i, [_vp, _u32]),
     "dtlg_set_l2_fetch_granularity": (_i, [_i, C.POINTER(_i)]),
+    "dtlg_autotune_probe": (_i, [_vp, _vp, _vp, _u32, _vp, _i, _vp, C.POINTER(ProbePlanS)]),
+    "dtlg_batch_autotune": (_i, [_vp, _i, _vp, C.POINTER(BatchPlanS)]),
+    "dtlg_batch_set_staging": (_i, [_vp, _i]),
+    "dtlg_batch_staged_count": (_u32, [_vp]),
     "dtlg_batch_prepare": (_i, [C.POINTER(BatchItemS), _u32, _i, C.POINTER(_vp)]),
     "dtlg_batch_run": (_i, [_vp, _vp]),
     "dtlg_batch_set_ctas_per_sm": (_i, [_vp, _i]),

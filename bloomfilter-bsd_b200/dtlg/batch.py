@@ -55,6 +55,21 @@ class Batch:
     def set_ctas_per_sm(self, n):
         check(lib().dtlg_batch_set_ctas_per_sm(self._h, int(n)), "batch_set_ctas_per_sm")
 
+    def autotune(self, reps=3):
+        """Times every (staging, CTAs per SM) choice and keeps the fastest;
+        returns {"staging", "ctas_per_sm", "ms"}."""
+        plan = _lib.BatchPlanS()
+        check(lib().dtlg_batch_autotune(self._h, int(reps), _stream(), C.byref(plan)), "batch_autotune")
+        return {"staging": plan.staging, "ctas_per_sm": plan.ctas_per_sm, "ms": plan.ms}
+
+    def set_staging(self, staging):
+        """0: build filters of up to 64 MiB range by range in shared memory
+        (default); 1: global atomic inserts only.  Results are identical."""
+        check(lib().dtlg_batch_set_staging(self._h, int(staging)), "batch_set_staging")
+
+    def staged_count(self):
+        return lib().dtlg_batch_staged_count(self._h)
+
     def kernel_count(self):
         return lib().dtlg_batch_kernel_count(self._h)
 

@@ -124,6 +124,20 @@ class filter_base:  # noqa: N801 (reference name)
         """Block-range passes of the two-kernel probe (0 = automatic)."""
         check(lib().dtlg_set_probe_passes(self._h, int(passes)), "set_probe_passes")
 
+    def autotune(self, filter_data, keys, reps=5):
+        """Times every probe plan on these keys and keeps the fastest for this
+        filter (the reference's calibrate(), blocked_bloomfilter_tune_impl.hpp:
+        162-268); returns {"mode", "variant", "passes", "ms", "gkeys_per_s"}."""
+        torch = _torch()
+        keys = as_device_keys(keys, filter_data.device)
+        pos = torch.empty(max(1, keys.numel()), dtype=torch.int32, device=keys.device)
+        plan = _lib.ProbePlanS()
+        check(lib().dtlg_autotune_probe(self._h, _dev_ptr(filter_data, "filter_data"), _dev_ptr(keys, "keys"),
+                                        keys.numel(), _dev_ptr(pos, "match_positions"), int(reps), _stream(),
+                                        C.byref(plan)), "autotune_probe")
+        return {"mode": plan.mode, "variant": plan.variant, "passes": plan.passes, "ms": plan.ms,
+                "gkeys_per_s": plan.gkeys_per_s}
+
     def alloc_filter_data(self, device="cuda"):
         """Zeroed filter words, as the facade allocates them (filter.hpp:113-119)."""
         torch = _torch()

@@ -144,6 +144,24 @@ int dtlg_probe_kernel_count(const dtlg_filter* f, uint32_t key_cnt);
  * process's context only and ends with it. */
 dtlg_status dtlg_set_l2_fetch_granularity(int bytes, int* in_effect);
 
+/* Probe autotuner, the counterpart of the reference's calibrate() tuners
+ * (blocked_bloomfilter_tune_impl.hpp:162-268, cuckoofilter_tune_impl.hpp:
+ * 118-225), which time SIMD unroll factors: times every probe plan (fused;
+ * bitmask kernel x register budget x block-range passes; partitioned for
+ * Bloom filters beyond 32 MiB) on these keys, `reps` runs each, keeps the
+ * fastest on the handle (as dtlg_set_probe_options / _passes would) and
+ * reports it.  All plans must agree on the match count (else DTLG_ERR_CUDA).
+ * match_positions: device, capacity >= n (scratch). */
+typedef struct dtlg_probe_plan {
+  int mode;                      /* 1 fused, 2 bitmask + compaction, 3 partitioned */
+  int variant;                   /* bitmask kernel register budget (-1: n/a) */
+  int passes;                    /* block-range passes of mode 2 (0: automatic) */
+  float ms;                      /* median time of one probe of the n keys */
+  float gkeys_per_s;
+} dtlg_probe_plan;
+dtlg_status dtlg_autotune_probe(dtlg_filter* f, const uint64_t* filter_words, const uint32_t* keys, uint32_t n,
+                                uint32_t* match_positions, int reps, dtlg_stream_t stream, dtlg_probe_plan* best);
+
 /* ---- probe without any allocation (no counterpart in the reference) ----
  * For callers that cannot call cudaMalloc -- a query engine whose device
  * memory is all owned by its own buffer manager, a plugin inside a host
@@ -191,6 +209,20 @@ dtlg_status dtlg_batch_prepare(const dtlg_batch_item* items, uint32_t n_items, i
 dtlg_status dtlg_batch_run(dtlg_batch* b, dtlg_stream_t stream);
 /* CTAs per SM of the persistent kernel (0 = as many as fit); set by the autotuner. */
 dtlg_status dtlg_batch_set_ctas_per_sm(dtlg_batch* b, int ctas_per_sm);
+/* Build staging: 0 = every filter of at most 2048 ranges of 32 KiB is built
+ * range by range in shared memory from key buckets (default), 1 = all filters
+ * insert with global atomics.  Results are identical; set by the autotuner. */
+dtlg_status dtlg_batch_set_staging(dtlg_batch* b, int staging);
+uint32_t dtlg_batch_staged_count(const dtlg_batch* b);
+/* Autotuner: times every (staging, CTAs per SM) choice over `reps` runs of
+ * the batch (runs are idempotent: OR-builds and the same match lists) and
+ * keeps the fastest. */
+typedef struct dtlg_batch_plan {
+  int staging;
+  int ctas_per_sm;
+  float ms;                      /* median time of one run */
+} dtlg_batch_plan;
+dtlg_status dtlg_batch_autotune(dtlg_batch* b, int reps, dtlg_stream_t stream, dtlg_batch_plan* best);
 int dtlg_batch_kernel_count(const dtlg_batch* b);
 uint32_t dtlg_batch_fallback_count(const dtlg_batch* b);
 void dtlg_batch_destroy(dtlg_batch* b);

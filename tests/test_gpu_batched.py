@@ -33,8 +33,8 @@ def make_batch(rng, n_filters):
     return cases
 
 
-@pytest.mark.parametrize("use_graph", [True, False])
-def test_batched_matches_oracle(use_graph):
+@pytest.mark.parametrize("use_graph,staging", [(True, 0), (False, 0), (True, 1)])
+def test_batched_matches_oracle(use_graph, staging):
     rng = np.random.default_rng(5 if use_graph else 6)
     cases = make_batch(rng, 40)
     items, refs = [], []
@@ -52,7 +52,9 @@ def test_batched_matches_oracle(use_graph):
                                torch.full((max(1, npb),), -1, dtype=torch.int32, device="cuda"),
                                torch.full((1,), -1, dtype=torch.int64, device="cuda"), off))
     b = Batch(items, use_graph=use_graph)
+    b.set_staging(staging)
     assert b.fallback_count() == sum(1 for c in cases if c[0] in OTHER)
+    assert (b.staged_count() > 0) == (staging == 0)
     for rep in range(3):  # later runs (graph replays) must not see earlier queue / status words
         for it in items:
             it.filter_data.zero_()
@@ -92,3 +94,61 @@ def test_batched_ctas_per_sm_tuning_keeps_results():
         for exp, it in zip(refs, items):
             n = int(it.match_cnt.item())
             assert np.array_equal(it.match_positions[:n].cpu().numpy().view(np.uint32), exp)
+
+
+def test_staged_build_with_skewed_keys_overflows_exactly():
+    """Keys that all fall into a few ranges overflow their buckets; the rest
+    of those keys takes the direct path and the words still match."""
+    rng = np.random.default_rng(8)
+    items, refs = [], []
+    for i, cfg in enumerate([(8, 8, 8, 1, 8), (8, 8, 8, 2, 8), (4, 16, 16, 4, 8), (4, 1, 1, 1, 4)]):
+        wb, w, s, z, k = cfg
+        n = 300000
+        few = keygen.build_keys(5, 70 + i)
+        bk = np.concatenate([np.repeat(few, n // 10), keygen.build_keys(n // 2, 80 + i)])
+        bk = bk[rng.permutation(len(bk))].astype(np.uint32)
+        m = (n * 12) | 1
+        f = F.construct(F.blocked_bloomfilter_config(k=k, word_size=wb, word_cnt_per_block=w, sector_cnt=s,
+                                                     zone_cnt=z), m)
+        ob = O.Bloom(wb, w, s, z, k, m)
+        rw = ob.alloc()
+        ob.insert(rw, bk)
+        pk = np.concatenate([few, keygen.probe_keys(n, 50000, 0.2, 90 + i)[0]]).astype(np.uint32)
+        refs.append((rw, ob.batch_contains(rw, pk, 3)))
+        items.append(BatchItem(f, f.alloc_filter_data(), dev(bk), dev(pk),
+                               torch.zeros(len(pk), dtype=torch.int32, device="cuda"),
+                               torch.zeros(1, dtype=torch.int64, device="cuda"), 3))
+    b = Batch(items)
+    assert b.staged_count() == len(items)
+    for _ in range(2):
+        for it in items:
+            it.filter_data.zero_()
+        b.run()
+        torch.cuda.synchronize()
+        for (rw, exp), it in zip(refs, items):
+            assert np.array_equal(it.filter_data.cpu().numpy().view(np.uint64), rw)
+            n = int(it.match_cnt.item())
+            assert np.array_equal(it.match_positions[:n].cpu().numpy().view(np.uint32), exp)
+
+
+def test_staged_build_ors_into_existing_words():
+    """batch_insert ORs into the caller's words: a staged build over a filter
+    that already holds keys equals building both key sets."""
+    wb, w, s, z, k = (8, 8, 8, 2, 8)
+    m = 1 << 22
+    f = F.construct(F.blocked_bloomfilter_config(k=k, word_size=wb, word_cnt_per_block=w, sector_cnt=s,
+                                                 zone_cnt=z), m)
+    ob = O.Bloom(wb, w, s, z, k, m)
+    a, c = keygen.build_keys(100000, 1), keygen.build_keys(200000, 2)
+    rw = ob.alloc()
+    ob.insert(rw, a)
+    data = torch.from_numpy(rw.copy().view(np.int64)).cuda()
+    ob.insert(rw, c)
+    pk = keygen.probe_keys(100000, 10000, 0.5, 1)[0]
+    item = BatchItem(f, data, dev(c), dev(pk), torch.zeros(len(pk), dtype=torch.int32, device="cuda"),
+                     torch.zeros(1, dtype=torch.int64, device="cuda"), 0)
+    b = Batch([item], use_graph=False)
+    assert b.staged_count() == 1
+    b.run()
+    torch.cuda.synchronize()
+    assert np.array_equal(data.cpu().numpy().view(np.uint64), rw)
