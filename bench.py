@@ -38,6 +38,10 @@ WORKLOADS = {
     "sectorized_dram_small": (8, 8, 8, 1, 8, 27, 16, 26, 0.10),
     "register_blocked": (4, 1, 1, 1, 4, 20, 16, 24, 0.10),
 }
+CUCKOO_WORKLOADS = {
+    # name: (bits per tag, tags per bucket, log2 n, load factor, log2 probes, hit ratio)
+    "cuckoo_dram": (16, 4, 26, 0.95, 28, 0.10),
+}
 SEED = 20240601
 
 
@@ -47,7 +51,8 @@ def parse():
     ap.add_argument("--steps", type=int, default=100)
     ap.add_argument("--warmup", type=int, default=5)
     ap.add_argument("--impl", choices=("dtlg", "reference"), default="dtlg")
-    ap.add_argument("--workload", choices=sorted(WORKLOADS) + ["batched512"], default="sectorized_dram")
+    ap.add_argument("--workload", choices=sorted(WORKLOADS) + sorted(CUCKOO_WORKLOADS) + ["batched512"],
+                    default="sectorized_dram")
     ap.add_argument("--no-cpu-baseline", action="store_true")
     ap.add_argument("--no-e2e", action="store_true")
     ap.add_argument("--probe-mode", type=int, default=0,
@@ -56,7 +61,30 @@ def parse():
     return ap.parse_args()
 
 
+def cuckoo_bits(n, t, b, lf):
+    """Table size in bits for n keys at load factor lf whose MAGIC bucket count
+    is odd: with an even one the reference's two-choice insert stalls near 75 %
+    occupancy (cuckoofilter_logic.hpp:216-252)."""
+    import dtlg
+    b0 = int(-(-n // (b * lf)))
+    for i in range(4096):
+        m = (b0 + i) * t * b
+        f = dtlg.cf(m, t, b)
+        if f.block_cnt() % 2 == 1 and f.is_magic() and f.block_cnt() * b * lf >= n:
+            return m
+    raise RuntimeError("no odd MAGIC bucket count found")
+
+
 def workload_config(name, n_gpus):
+    if name in CUCKOO_WORKLOADS:
+        t, b, ln, lf, lp, h = CUCKOO_WORKLOADS[name]
+        return {
+            "workload": name, "filter": f"cuckoo t={t} b={b} (MAGIC, odd bucket count)", "load_factor": lf,
+            "build_keys": 1 << ln, "probe_keys_per_gpu": 1 << lp, "global_batch": (1 << lp) * n_gpus,
+            "hit_ratio": h, "filter_bytes": int(-(-(1 << ln) // (b * lf))) * t * b // 8,
+            "parallelism": f"dp{n_gpus} (replicated filter, sharded probes)",
+            "l2_flush": "inputs larger than L2 (keys 4 B/key x probes + filter words)",
+        }
     wb, w, s, z, k, ln, bpk, lp, h = WORKLOADS[name]
     return {
         "workload": name,
@@ -140,7 +168,7 @@ def load_peaks():
 
 
 # ---------------------------------------------------------------------------
-def cpu_reference_probe(words_np, cfg, n_build, probe_np, threads, budget_s, want_kind="reference"):
+def cpu_reference_probe(words_np, cfg, m, probe_np, threads, budget_s, want_kind="reference"):
     """The reference's own SIMD batch_contains (oracle/_ref) -- or, if that
     library is absent, the C restatement -- on a bounded sample of the probe
     stream, all host threads.  Returns (keys/s, kind, sample keys, count)."""
@@ -148,16 +176,18 @@ def cpu_reference_probe(words_np, cfg, n_build, probe_np, threads, budget_s, wan
     import numpy as np
 
     import oracle as O
-    wb, w, s, z, k = cfg
-    m = n_build * 16
     ref = O.try_reflib() if want_kind == "reference" else None
     out = np.empty(len(probe_np) + 64, dtype=np.uint32)
+    f = None
     if ref is not None:
-        f = ref.bloom(wb, w, s, z, k, m)
+        f = ref.cuckoo(cfg[1], cfg[2], m) if cfg[0] == "cuckoo" else ref.bloom(*cfg, m)
+    if f is not None:
         kind = "reference"
         run = lambda keys: f.batch_contains_mt(words_np, keys, threads, unroll=1, out=out)  # noqa: E731
     else:
-        f = O.Bloom(wb, w, s, z, k, m)
+        if cfg[0] == "cuckoo":
+            raise RuntimeError("the reference build lacks this cuckoo config")
+        f = O.Bloom(*cfg, m)
         kind = "port"
         run = lambda keys: f.batch_contains_mt(words_np, keys, threads)  # noqa: E731
     # size the sample so one pass takes about budget_s
@@ -173,7 +203,7 @@ def cpu_reference_probe(words_np, cfg, n_build, probe_np, threads, budget_s, wan
         cnt = run(probe_np[:n])
         dt = time.perf_counter() - t0
         best = dt if best is None else min(best, dt)
-    return n / best, kind, n, cnt, (ref.variant if ref is not None else "c")
+    return n / best, kind, n, cnt, (ref.variant if kind == "reference" else "c")
 
 
 # ---------------------------------------------------------------------------
@@ -193,16 +223,28 @@ def run_dtlg(args):
         from datetime import timedelta
         dist.init_process_group("nccl", timeout=timedelta(seconds=300), device_id=torch.device("cuda", local))
 
-    wb, w, s, z, k, ln, bpk, lp, hit = WORKLOADS[args.workload]
-    n_build, P = 1 << ln, 1 << lp
-    m = n_build * bpk
-    cfg = dtlg.blocked_bloomfilter_config(k=k, word_size=wb, word_cnt_per_block=w, sector_cnt=s, zone_cnt=z)
-    f = dtlg.construct(cfg, m)
+    if args.workload in CUCKOO_WORKLOADS:
+        tag_bits, slots, ln, lf, lp, hit = CUCKOO_WORKLOADS[args.workload]
+        n_build, P = 1 << ln, 1 << lp
+        m = cuckoo_bits(n_build, tag_bits, slots, lf)
+        f = dtlg.cf(m, tag_bits, slots)
+        block_bytes, sectors = (tag_bits * slots + 7) // 8, 2   # two buckets, 8-byte aligned: one sector each
+    else:
+        wb, w, s, z, k, ln, bpk, lp, hit = WORKLOADS[args.workload]
+        n_build, P = 1 << ln, 1 << lp
+        m = n_build * bpk
+        cfg = dtlg.blocked_bloomfilter_config(k=k, word_size=wb, word_cnt_per_block=w, sector_cnt=s, zone_cnt=z)
+        f = dtlg.construct(cfg, m)
+        block_bytes = w * wb
+        sectors = -(-block_bytes // 32)
     f.set_probe_options(args.probe_mode, -1)
     f.set_probe_passes(args.probe_passes)
     words = f.alloc_filter_data()
     bk = keygen.build_keys_torch(n_build, SEED)
-    assert f.batch_insert(words, bk)
+    assert f.batch_insert(words, bk), "build failed"
+    if args.workload in CUCKOO_WORKLOADS:
+        occupied = f.count_occupied_slots(words)
+        assert occupied == n_build, (occupied, n_build)
     del bk
     # this rank's slice of the probe stream; positions are global (offset)
     start = rank * P
@@ -259,8 +301,8 @@ def run_dtlg(args):
 
     # roofline of the probe kernel (one launch per step)
     mu = count / P
-    dram_resident = m // 8 > 126 * 2 ** 20
-    S = -(-(w * wb) // 32) if dram_resident else 0
+    dram_resident = f.size_in_bytes() > torch.cuda.get_device_properties(local).L2_cache_size
+    S = sectors if dram_resident else 0
     alg_bytes_per_key = 4 + 4 * mu + 32 * S
     launch_ms = statistics.mean(per_launch_ms)
     achieved = P * alg_bytes_per_key / (launch_ms / 1e3) / 1e9
@@ -333,8 +375,8 @@ def run_dtlg(args):
             threads = len(os.sched_getaffinity(0))
             words_np = words.cpu().numpy().view(np.uint64)
             probe_np = keys.cpu().numpy().view(np.uint32)
-            rate, kind, n, c, variant = cpu_reference_probe(words_np, (wb, w, s, z, k), n_build, probe_np,
-                                                            threads, budget_s=4.0)
+            fcfg = ("cuckoo", tag_bits, slots) if args.workload in CUCKOO_WORKLOADS else (wb, w, s, z, k)
+            rate, kind, n, c, variant = cpu_reference_probe(words_np, fcfg, m, probe_np, threads, budget_s=4.0)
             result["cpu_baseline"] = {"value": round(rate / 1e9, 4), "unit": "Gkeys/s", "cores": threads,
                                       "kind": kind,
                                       "sample": f"first {n} probe keys of this workload, best of 2, "
@@ -369,22 +411,39 @@ def run_reference(args):
         print(json.dumps({"impl": "reference", "unavailable": "oracle/_ref (the reference compiled from its "
                                                                "sources) is not built on this machine"}))
         return
-    wb, w, s, z, k, ln, bpk, lp, hit = WORKLOADS[args.workload]
-    n_build, P = 1 << ln, 1 << lp
-    m = n_build * bpk
     threads = len(os.sched_getaffinity(0))
-    f = ref.bloom(wb, w, s, z, k, m)
-    words = np.zeros((f.word_cnt * wb + 7) // 8, dtype=np.uint64)
     chunk = 1 << 24
+    if args.workload in CUCKOO_WORKLOADS:
+        t, b, ln, lf, lp, hit = CUCKOO_WORKLOADS[args.workload]
+        n_build, P = 1 << ln, 1 << lp
+        m = cuckoo_bits(n_build, t, b, lf)
+        f = ref.cuckoo(t, b, m)
+        # table words plus the victim record the reference keeps after them
+        words = np.zeros((f.word_cnt * 4 + 64) // 8, dtype=np.uint64)
+    else:
+        wb, w, s, z, k, ln, bpk, lp, hit = WORKLOADS[args.workload]
+        n_build, P = 1 << ln, 1 << lp
+        m = n_build * bpk
+        f = ref.bloom(wb, w, s, z, k, m)
+        words = np.zeros((f.word_cnt * wb + 7) // 8, dtype=np.uint64)
+    if f is None:
+        print(json.dumps({"impl": "reference", "unavailable": "this configuration is not instantiated in the "
+                                                               "reference build (oracle/_ref)"}))
+        return
     with ThreadPoolExecutor(max(1, min(threads, 32))) as ex:
-        parts = list(ex.map(lambda b: keygen.build_keys(min(chunk, n_build - b), SEED, start=b),
+        parts = list(ex.map(lambda c0: keygen.build_keys(min(chunk, n_build - c0), SEED, start=c0),
                             range(0, n_build, chunk)))
         bk = np.concatenate(parts)
-        f.insert_mt(words, bk, threads) if z == 1 else f.insert(words, bk)
+        if args.workload in CUCKOO_WORKLOADS:
+            assert f.insert(words, bk), "reference cuckoo build failed"   # its inserts are not thread-safe
+        elif z == 1:
+            f.insert_mt(words, bk, threads)
+        else:
+            f.insert(words, bk)
         del bk, parts
         # probe sample: as many keys as take ~2 s per step on this host
         probe = np.concatenate(list(ex.map(
-            lambda b: keygen.probe_keys(n_build, min(chunk, P - b), hit, SEED, start=b)[0],
+            lambda c0: keygen.probe_keys(n_build, min(chunk, P - c0), hit, SEED, start=c0)[0],
             range(0, min(P, 1 << 26), chunk))))
     out = np.empty(len(probe) + 64, dtype=np.uint32)
     t0 = time.perf_counter()
@@ -470,6 +529,7 @@ def run_batched(args):
     stream = torch.cuda.current_stream()
     L = dtlg.lib()
     batch = Batch(items, use_graph=True)
+    tuned = batch.autotune(reps=2)   # staging and CTAs per SM, picked by timing
 
     def batched_step():
         arena.zero_()
@@ -538,6 +598,8 @@ def run_batched(args):
         "speedup_vs_per_filter": round(ms_per_filter / ms_batched, 3),
         "gpu_launches": steps * (batch.kernel_count()),
         "fallback_filters": batch.fallback_count(),
+        "autotuned": {"staging": tuned["staging"], "ctas_per_sm": tuned["ctas_per_sm"],
+                      "staged_filters": batch.staged_count()},
         "clocks": clk,
     }
     print(json.dumps(result), flush=True)

@@ -168,8 +168,17 @@ __device__ __forceinline__ void build_range(const BatchDesc& d, uint32_t rg, uns
     Word* base = s_w + static_cast<uint64_t>(block_index(key * mul_const(0), d.addr) - blk0) * kW;
     static_for<BloomOps<Cfg>::kS.ng>([&](auto G) {
       constexpr int g = decltype(G)::value;
-      atomic_or_word<Word>(base + BloomOps<Cfg>::template group_word<g>(key),
-                           BloomOps<Cfg>::template group_mask<g>(key));
+      Word* p = base + BloomOps<Cfg>::template group_word<g>(key);
+      const Word m = BloomOps<Cfg>::template group_mask<g>(key);
+      if constexpr (sizeof(Word) == 8) {
+        // 32-bit shared-memory atomics on the halves that have bits to set
+        uint32_t* p32 = reinterpret_cast<uint32_t*>(p);
+        const uint32_t lo = static_cast<uint32_t>(m), hi = static_cast<uint32_t>(m >> 32);
+        if (lo) atomicOr(p32, lo);
+        if (hi) atomicOr(p32 + 1, hi);
+      } else {
+        atomicOr(reinterpret_cast<uint32_t*>(p), static_cast<uint32_t>(m));
+      }
     });
   }
   __syncthreads();
