@@ -385,6 +385,12 @@ def run_dtlg(args):
         except Exception as e:  # the baseline is reported, never required
             result["cpu_baseline"] = {"value": None, "error": str(e)[:200]}
 
+    if world > 1:
+        # the probe's one exchange: every rank's match count (places its
+        # positions in the concatenated list)
+        from dtlg.shard import gather_counts, output_offsets
+        counts = gather_counts(count)
+        result["match_count_total"] = output_offsets(counts)[1]
     if rank == 0:
         print(json.dumps(result), flush=True)
     if world > 1:

@@ -295,6 +295,14 @@ dtlg_status dtlg_mlp_train(dtlg_mlp* m, const float* x, const float* t, const fl
 dtlg_status dtlg_mlp_choose(dtlg_mlp* m, const float* x, uint32_t n, uint32_t n_cand, float* y_scratch,
                             int32_t* choice, float* aux, dtlg_stream_t stream);
 
+/* ---- sharded builds (several GPUs) ----
+ * dst[i] |= src[j * src_stride + i] for i < n_words, j < n_src (device
+ * pointers): the OR that combines partial Bloom filters built from shards of
+ * the keys.  Counterpart: the reference replicates a finished filter per NUMA
+ * node (filter.hpp:128-152) and has no sharded build. */
+dtlg_status dtlg_or_words(uint64_t* dst, const uint64_t* src, uint64_t n_words, uint32_t n_src, uint64_t src_stride,
+                          dtlg_stream_t stream);
+
 /* ---- single keys: filter_base::insert / contains (filter_base.hpp:22,32) ---- */
 dtlg_status dtlg_insert(const dtlg_filter* f, uint64_t* filter_words, uint32_t key, dtlg_stream_t stream);
 dtlg_status dtlg_contains(const dtlg_filter* f, const uint64_t* filter_words, uint32_t key,
