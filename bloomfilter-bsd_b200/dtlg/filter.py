@@ -296,6 +296,17 @@ class filter:  # noqa: N801 -- dtl::filter::filter (filter.hpp:35-261)
         self.filter_instance = construct(config, m)
         self.filter_data = self.filter_instance.alloc_filter_data(device)
 
+    @staticmethod
+    def for_workload(n, work_ns, fpr_target=0.1, hit_ratio=0.0, l2_resident=False, method="mlp", device="cuda"):
+        """The filter the cost model picks for n build keys and work_ns of
+        downstream work per passing tuple -- construct(n, tw, ...) of the
+        reference (filter.hpp:76-82), which reads its skyline matrix.  method:
+        "mlp" (the trained network, GPU), "skyline" (the reference's cached
+        lookup) or "exhaustive" (the calibrated search)."""
+        from .model.planner import shared_planner
+        cfg, m = shared_planner().config_for(n, fpr_target, hit_ratio, work_ns, l2_resident, method)
+        return filter(cfg, m, device)
+
     def insert(self, keys):
         torch = _torch()
         if isinstance(keys, torch.Tensor) and keys.is_cuda:

@@ -129,6 +129,17 @@ class Planner:
         return c.config(), m_bits
 
 
+_SHARED = None
+
+
+def shared_planner():
+    """One Planner per process over the packaged calibration data and weights."""
+    global _SHARED
+    if _SHARED is None:
+        _SHARED = Planner.load()
+    return _SHARED
+
+
 def regret_report(planner, queries, best_cost, methods=("mlp", "skyline", "exhaustive")):
     out = {}
     for meth in methods:

@@ -132,3 +132,17 @@ def test_planner_config_builds_a_filter_meeting_the_target():
         pos = torch.empty(pk.numel(), dtype=torch.int32, device="cuda")
         fpr = f.batch_contains(data, pk, pk.numel(), pos, 0) / pk.numel()
         assert fpr <= target * 1.3, (cfg, m_bits, fpr)
+
+
+@pytest.mark.skipif(not (os.path.exists(DEFAULT_PATH) and os.path.exists(DEFAULT_WEIGHTS)),
+                    reason="no calibration data / trained weights")
+def test_facade_for_workload_builds_and_probes():
+    import dtlg
+    from dtlg import keygen
+    for method in ("mlp", "skyline", "exhaustive"):
+        f = dtlg.filter.for_workload(1 << 16, work_ns=100.0, fpr_target=1e-3, hit_ratio=0.2, method=method)
+        f.insert(keygen.build_keys_torch(1 << 16, 4))
+        pk, member = keygen.probe_keys_torch(1 << 16, 1 << 18, 0.2, 4)
+        pos = torch.empty(pk.numel(), dtype=torch.int32, device="cuda")
+        cnt = f.probe()(pk, pos, 0)
+        assert cnt >= int(member.sum().item())
