@@ -149,7 +149,8 @@ class ClockSampler:
 
 
 def load_traffic_profile():
-    """DRAM bytes per probed key of the probe kernel from the committed ncu summary."""
+    """DRAM bytes per probed key of one probe step, per workload, from the
+    committed ncu summary (profiles/probe_traffic.json)."""
     path = os.path.join(ROOT, "profiles", "probe_traffic.json")
     try:
         with open(path) as f:
@@ -309,8 +310,8 @@ def run_dtlg(args):
     peak, peak_kind = load_peaks()
     prof = load_traffic_profile()
     traffic = None
-    if prof and prof.get("workload") == args.workload:
-        traffic = prof["dram_bytes_per_key"] * P
+    if prof and isinstance(prof.get(args.workload), dict) and args.probe_mode == 0 and args.probe_passes == 0:
+        traffic = round(prof[args.workload]["dram_bytes_per_key"] * P)
 
     result = {
         "metric": "probe Gkeys/s (batch_contains, ascending match positions)",
