@@ -3,12 +3,15 @@
 // A query plan with one filter per partition or semi-join has hundreds of
 // filters of very uneven size; launching a build and a probe per filter spends
 // most of the time on launch latency and tail effects.  Here all filters are
-// described by a table, and one persistent kernel works through three queues:
+// described by a table, and one persistent kernel works through a queue of three kinds of items:
 //
-//   build queue: tiles of 4096 build keys, over all filters;
-//   range queue: (filter, block range) items of staged filters;
-//   probe queue: tiles of 4096 probe keys, over all filters, each filter's
-//                tiles in order (per-filter ordered compaction).
+//   build tiles: 4096 build keys of one filter;
+//   range items: one block range of a staged filter;
+//   probe tiles: 4096 probe keys of one filter, each filter's tiles in order
+//                (per-filter ordered compaction).
+//
+// The items form one queue: all build tiles, then all range items, then all
+// probe tiles, each kind in filter order.
 //
 // A build tile either inserts its keys with global atomic ORs (direct
 // filters), or -- for a staged filter -- only sorts them into per-range
@@ -21,12 +24,11 @@
 // turns them into streaming traffic.  A bucket that fills up sends the rest
 // of its keys down the direct path, so any key distribution is built exactly.
 //
-// CTAs drain the queues in order.  A range item of filter f waits until all
+// CTAs take items in queue order.  A range item of filter f waits until all
 // of f's build tiles are done; a probe tile of f waits until f is built (all
-// its ranges, or all its build tiles when direct).  The waits are bounded and
-// cannot deadlock: by the time an item of a later queue is handed out, every
-// item of the earlier queues has been taken by a running CTA, and those only
-// wait on queues earlier still.  The per-filter look-back of the ordered
+// its ranges, or all its build tiles when direct).  Every item waits only on
+// items earlier in the queue, which running CTAs have already taken and which
+// themselves wait only on earlier items; so the bounded waits cannot deadlock.  The per-filter look-back of the ordered
 // compaction is the one of probe.cuh.  Filter words are read with coherent
 // loads, because they were written earlier in the same kernel.
 #pragma once
@@ -61,18 +63,20 @@ struct BatchDesc {
   unsigned int* cursor;         // per range: keys sorted in so far (zeroed)
 };
 
+// Work items of the single queue: x = kind << 30 | filter, y = the kind's index.
+constexpr uint32_t kItemBuild = 0;   // y: the filter's build tile
+constexpr uint32_t kItemRange = 1;   // y: the range of a staged filter
+constexpr uint32_t kItemProbe = 2;   // y: the global probe tile (look-back word)
+
 struct BatchArgs {
   const BatchDesc* desc;
   uint32_t n_filters;
-  const uint32_t* build_map;    // global build tile -> filter
-  const uint32_t* probe_map;    // global probe tile -> filter
-  uint32_t n_build_tiles, n_probe_tiles;
+  const uint2* items;           // the queue, in hand-out order
+  uint32_t n_items;
   unsigned long long* status;   // one look-back word per global probe tile (zeroed)
   unsigned int* built;          // per filter: build tiles done (zeroed)
   unsigned int* ranges_built;   // per filter: range items done (zeroed)
-  const uint2* range_items;     // range queue: (filter, range)
-  uint32_t n_range_items;
-  unsigned int* ctl;            // [0] build, [1] probe, [3] range queue heads, [2] error word (zeroed)
+  unsigned int* ctl;            // [0] queue head, [2] error word (zeroed)
 };
 
 #ifdef __CUDACC__
@@ -107,14 +111,59 @@ __device__ __forceinline__ void wait_counter(const unsigned int* ctr, uint32_t n
   __syncthreads();
 }
 
-// Sorts one build tile of a staged filter into its range buckets.
+// Block-wide exclusive scan of v[0..n) in place (n <= kBatchMaxRanges, 8
+// entries per thread); returns the total.
+__device__ __forceinline__ uint32_t block_exclusive_scan(uint32_t* v, uint32_t n, uint32_t* s_warp) {
+  constexpr uint32_t kPer = kBatchMaxRanges / kBatchThreads;
+  const uint32_t lane = threadIdx.x & 31u, warp = threadIdx.x >> 5;
+  const uint32_t i0 = threadIdx.x * kPer;
+  uint32_t x[kPer], sum = 0;
+#pragma unroll
+  for (uint32_t j = 0; j < kPer; j++) {
+    x[j] = i0 + j < n ? v[i0 + j] : 0u;
+    sum += x[j];
+  }
+  uint32_t incl = sum;
+#pragma unroll
+  for (int d = 1; d < 32; d <<= 1) {
+    const uint32_t t = __shfl_up_sync(0xffffffffu, incl, d);
+    if (lane >= static_cast<uint32_t>(d)) incl += t;
+  }
+  if (lane == 31) s_warp[warp] = incl;
+  __syncthreads();
+  uint32_t before = 0, total = 0;
+#pragma unroll
+  for (uint32_t w = 0; w < kBatchThreads / 32; w++) {
+    const uint32_t t = s_warp[w];
+    before += w < warp ? t : 0u;
+    total += t;
+  }
+  uint32_t run = before + incl - sum;
+#pragma unroll
+  for (uint32_t j = 0; j < kPer; j++) {
+    if (i0 + j < n) v[i0 + j] = run;
+    run += x[j];
+  }
+  __syncthreads();
+  return total;
+}
+
+// Sorts one build tile of a staged filter into its range buckets.  The tile
+// is first ordered by range in shared memory, so that each range's run of
+// keys goes to its bucket as consecutive (coalesced) stores; one atomic per
+// (tile, range) reserves the run's place in the bucket.
+//   smem: s_cnt / s_gbase [kBatchMaxRanges] + s_keys [kBatchTile] = 32 KiB.
 template <class Cfg>
-__device__ __forceinline__ void scatter_tile(const BatchDesc& d, uint64_t k0, uint32_t* s_hist, uint32_t* s_base) {
+__device__ __forceinline__ void scatter_tile(const BatchDesc& d, uint64_t k0, unsigned char* smem,
+                                             uint32_t* s_warp) {
   constexpr int kRounds = kBatchTile / (kBatchThreads * 4);
-  for (uint32_t i = threadIdx.x; i < d.n_ranges; i += kBatchThreads) s_hist[i] = 0u;
+  uint32_t* s_cnt = reinterpret_cast<uint32_t*>(smem);       // counts, then tile-local run starts
+  uint32_t* s_gbase = s_cnt + kBatchMaxRanges;                // bucket position of each run
+  uint32_t* s_keys = s_gbase + kBatchMaxRanges;               // the tile ordered by range
+  for (uint32_t i = threadIdx.x; i < d.n_ranges; i += kBatchThreads) s_cnt[i] = 0u;
   __syncthreads();
   const uint4* k4 = reinterpret_cast<const uint4*>(d.build_keys + k0);
-  uint32_t key[kRounds * 4], slot[kRounds * 4];  // slot: range << 12 | index within the tile's share
+  uint32_t key[kRounds * 4], slot[kRounds * 4];  // slot: range << 12 | rank within the tile's run
 #pragma unroll
   for (int r = 0; r < kRounds; r++) {
     const uint64_t i0 = static_cast<uint64_t>(r) * (kBatchThreads * 4) + threadIdx.x * 4u;
@@ -127,25 +176,29 @@ __device__ __forceinline__ void scatter_tile(const BatchDesc& d, uint64_t k0, ui
       slot[r * 4 + q] = 0xffffffffu;
       if (k0 + i0 + q < d.n_build) {
         const uint32_t rg = block_index(k[q] * mul_const(0), d.addr) >> d.range_shift;
-        slot[r * 4 + q] = (rg << 12) | atomicAdd(&s_hist[rg], 1u);
+        slot[r * 4 + q] = (rg << 12) | atomicAdd(&s_cnt[rg], 1u);
       }
     }
   }
   __syncthreads();
   for (uint32_t i = threadIdx.x; i < d.n_ranges; i += kBatchThreads) {
-    const uint32_t h = s_hist[i];
-    s_base[i] = h ? atomicAdd(&d.cursor[i], h) : 0u;
+    const uint32_t h = s_cnt[i];
+    s_gbase[i] = h ? atomicAdd(&d.cursor[i], h) : 0u;
   }
   __syncthreads();
+  const uint32_t n_valid = block_exclusive_scan(s_cnt, d.n_ranges, s_warp);
 #pragma unroll
-  for (int j = 0; j < kRounds * 4; j++) {
-    if (slot[j] == 0xffffffffu) continue;
-    const uint32_t rg = slot[j] >> 12;
-    const uint32_t pos = s_base[rg] + (slot[j] & 0xfffu);
+  for (int j = 0; j < kRounds * 4; j++)
+    if (slot[j] != 0xffffffffu) s_keys[s_cnt[slot[j] >> 12] + (slot[j] & 0xfffu)] = key[j];
+  __syncthreads();
+  for (uint32_t sl = threadIdx.x; sl < n_valid; sl += kBatchThreads) {
+    const uint32_t kk = s_keys[sl];
+    const uint32_t rg = block_index(kk * mul_const(0), d.addr) >> d.range_shift;
+    const uint32_t pos = s_gbase[rg] + (sl - s_cnt[rg]);
     if (pos < d.bucket_cap) {
-      d.bucket[static_cast<uint64_t>(rg) * d.bucket_cap + pos] = key[j];
+      d.bucket[static_cast<uint64_t>(rg) * d.bucket_cap + pos] = kk;
     } else {
-      BloomOps<Cfg>::insert(d.words, key[j], d.addr);  // bucket full: direct path
+      BloomOps<Cfg>::insert(d.words, kk, d.addr);  // bucket full: direct path
     }
   }
 }
@@ -211,71 +264,60 @@ __global__ void __launch_bounds__(kBatchThreads) batched_kernel(const __grid_con
       if (a.desc[f].n_probe == 0) *a.desc[f].count_out = 0ull;
   }
 
-  // ---- build queue ----
-  for (;;) {
-    if (threadIdx.x == 0) s_tile = atomicAdd(&a.ctl[0], 1u);
-    __syncthreads();
-    const uint32_t tile = s_tile;
-    __syncthreads();
-    if (tile >= a.n_build_tiles) break;
-    const uint32_t f = a.build_map[tile];
-    const BatchDesc& d = a.desc[f];
-    const uint64_t k0 = static_cast<uint64_t>(tile - d.build_tile0) * kBatchTile;
-    dispatch_cfg<Cfgs...>(d.cfg, [&](auto c) {
-      using Cfg = decltype(c);
-      if (d.staged) {
-        uint32_t* s_hist = reinterpret_cast<uint32_t*>(s_dyn);
-        scatter_tile<Cfg>(d, k0, s_hist, s_hist + kBatchMaxRanges);
-        return;
-      }
-      const uint4* k4 = reinterpret_cast<const uint4*>(d.build_keys + k0);
-#pragma unroll
-      for (int r = 0; r < kRounds; r++) {
-        const uint64_t i0 = static_cast<uint64_t>(r) * (kBatchThreads * 4) + threadIdx.x * 4u;
-        if (k0 + i0 >= d.n_build) continue;
-        const uint4 kv = __ldcs(k4 + (i0 >> 2));
-        const uint32_t k[4] = {kv.x, kv.y, kv.z, kv.w};
-#pragma unroll
-        for (int q = 0; q < 4; q++)
-          if (k0 + i0 + q < d.n_build) BloomOps<Cfg>::insert(d.words, k[q], d.addr);
-      }
-    });
-    __syncthreads();
-    if (threadIdx.x == 0) {
-      __threadfence();
-      atomicAdd(&a.built[f], 1u);
-    }
-  }
-
-  // ---- range queue (staged filters) ----
-  for (;;) {
-    if (threadIdx.x == 0) s_tile = atomicAdd(&a.ctl[3], 1u);
-    __syncthreads();
-    const uint32_t item = s_tile;
-    __syncthreads();
-    if (item >= a.n_range_items) break;
-    const uint2 fr = a.range_items[item];
-    const BatchDesc& d = a.desc[fr.x];
-    wait_counter(&a.built[fr.x], d.n_build_tiles, &a.ctl[2]);
-    dispatch_cfg<Cfgs...>(d.cfg, [&](auto c) { build_range<decltype(c)>(d, fr.y, s_dyn); });
-    __syncthreads();
-    if (threadIdx.x == 0) {
-      __threadfence();
-      atomicAdd(&a.ranges_built[fr.x], 1u);
-    }
-  }
-
-  // ---- probe queue ----
   ProbeArgs lb{};  // look-back state: status words + error word
   lb.status = a.status;
   lb.err = &a.ctl[2];
   for (;;) {
-    if (threadIdx.x == 0) s_tile = atomicAdd(&a.ctl[1], 1u);
+    if (threadIdx.x == 0) s_tile = atomicAdd(&a.ctl[0], 1u);
     __syncthreads();
-    const uint32_t tile = s_tile;
-    if (tile >= a.n_probe_tiles) break;
-    const uint32_t f = a.probe_map[tile];
+    const uint32_t item = s_tile;
+    __syncthreads();
+    if (item >= a.n_items) break;
+    const uint2 it = a.items[item];
+    const uint32_t kind = it.x >> 30, f = it.x & 0x3fffffffu;
     const BatchDesc& d = a.desc[f];
+
+    if (kind == kItemBuild) {
+      const uint64_t k0 = static_cast<uint64_t>(it.y) * kBatchTile;
+      dispatch_cfg<Cfgs...>(d.cfg, [&](auto c) {
+        using Cfg = decltype(c);
+        if (d.staged) {
+          scatter_tile<Cfg>(d, k0, s_dyn, s_wtot);
+          return;
+        }
+        const uint4* k4 = reinterpret_cast<const uint4*>(d.build_keys + k0);
+#pragma unroll
+        for (int r = 0; r < kRounds; r++) {
+          const uint64_t i0 = static_cast<uint64_t>(r) * (kBatchThreads * 4) + threadIdx.x * 4u;
+          if (k0 + i0 >= d.n_build) continue;
+          const uint4 kv = __ldcs(k4 + (i0 >> 2));
+          const uint32_t k[4] = {kv.x, kv.y, kv.z, kv.w};
+#pragma unroll
+          for (int q = 0; q < 4; q++)
+            if (k0 + i0 + q < d.n_build) BloomOps<Cfg>::insert(d.words, k[q], d.addr);
+        }
+      });
+      __syncthreads();
+      if (threadIdx.x == 0) {
+        __threadfence();
+        atomicAdd(&a.built[f], 1u);
+      }
+      continue;
+    }
+
+    if (kind == kItemRange) {
+      wait_counter(&a.built[f], d.n_build_tiles, &a.ctl[2]);
+      dispatch_cfg<Cfgs...>(d.cfg, [&](auto c) { build_range<decltype(c)>(d, it.y, s_dyn); });
+      __syncthreads();
+      if (threadIdx.x == 0) {
+        __threadfence();
+        atomicAdd(&a.ranges_built[f], 1u);
+      }
+      continue;
+    }
+
+    // kItemProbe
+    const uint32_t tile = it.y;
     const uint32_t local = tile - d.probe_tile0;
     if (d.staged) {
       wait_counter(&a.ranges_built[f], d.n_ranges, &a.ctl[2]);
