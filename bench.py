@@ -54,6 +54,8 @@ def parse():
     ap.add_argument("--workload", choices=sorted(WORKLOADS) + sorted(CUCKOO_WORKLOADS) + ["batched512"],
                     default="sectorized_dram")
     ap.add_argument("--no-cpu-baseline", action="store_true")
+    ap.add_argument("--batch-filters", type=int, default=512, help="batched512: number of filters")
+    ap.add_argument("--batch-max-log2", type=int, default=24, help="batched512: log2 of the largest n / probes")
     ap.add_argument("--no-e2e", action="store_true")
     ap.add_argument("--probe-mode", type=int, default=0,
                     help="0 auto, 1 fused, 2 bitmask + block-range passes, 3 partitioned")
@@ -484,17 +486,18 @@ def run_reference(args):
 BATCH_CONFIGS = [(8, 8, 8, 2, 8), (8, 8, 8, 4, 8), (4, 16, 16, 2, 8), (4, 16, 16, 4, 8), (8, 8, 8, 1, 8)]
 
 
-def batched_plan(n_filters=512, seed=4242):
+def batched_plan(n_filters=512, seed=4242, max_log2=24):
     """512 filters: config from the zoned (2/4 zones, u64 w=8 and u32 w=16) and
     sectorized (u64 w=8 s=8) set, n log-uniform over 2^10..2^24, probes
-    log-uniform over 2^12..2^24 at 5 % hits, 8/12/16 bits per key."""
+    log-uniform over 2^12..2^24 at 5 % hits, 8/12/16 bits per key (a smaller
+    n_filters / max_log2 gives the small case that profilers capture)."""
     import numpy as np
     rng = np.random.default_rng(seed)
     plan = []
     for i in range(n_filters):
         cfg = BATCH_CONFIGS[int(rng.integers(0, len(BATCH_CONFIGS)))]
-        n = int(2 ** rng.uniform(10, 24))
-        p = int(2 ** rng.uniform(12, 24))
+        n = int(2 ** rng.uniform(10, max_log2))
+        p = int(2 ** rng.uniform(12, max_log2))
         bpk = int(rng.choice([8, 12, 16]))
         plan.append((cfg, n * bpk, n, p))
     return plan
@@ -511,7 +514,7 @@ def run_batched(args):
     from dtlg import keygen
     from dtlg.batch import Batch, BatchItem
     torch.cuda.set_device(int(os.environ.get("LOCAL_RANK", "0")))
-    plan = batched_plan()
+    plan = batched_plan(args.batch_filters, max_log2=args.batch_max_log2)
     items = []
     total_words = 0
     filters = []
