@@ -199,10 +199,21 @@ void partition_ranges(const dtlg_filter* f, uint32_t* range_log2, uint32_t* n_ra
   *n_ranges = static_cast<uint32_t>((nb + (1ull << L) - 1) >> L);
 }
 
-// Enqueues the probe of `keys[0..n)`; the count goes to count_dev.
+// Payload columns copied along with the match positions (probe -> gather).
+struct GatherSpec {
+  uint32_t n_cols;
+  uint32_t col_bytes[kMaxGatherCols];
+  const void* cols[kMaxGatherCols];
+  void* out_cols[kMaxGatherCols];
+};
+
+// Enqueues the probe of `keys[0..n)`; the count goes to count_dev.  With
+// `gather`, the compaction also copies the matching rows of the payload
+// columns (the fused single-kernel plan has no compaction pass of its own,
+// so gathers always take the bitmask plan).
 dtlg_status launch_probe(const dtlg_filter* f, const uint64_t* words, const uint32_t* keys, uint32_t n,
                          uint32_t* out, uint32_t offset, unsigned long long* count_dev, void* ws,
-                         size_t ws_bytes, cudaStream_t stream) {
+                         size_t ws_bytes, cudaStream_t stream, const GatherSpec* gather = nullptr) {
   DeviceState* ds = nullptr;
   dtlg_status st = device_state(&ds);
   if (st) return st;
@@ -212,7 +223,8 @@ dtlg_status launch_probe(const dtlg_filter* f, const uint64_t* words, const uint
   }
   const uint32_t pre = static_cast<uint32_t>((reinterpret_cast<uintptr_t>(keys) & 15u) >> 2);
   const uint64_t n_phys = static_cast<uint64_t>(n) + pre;
-  const int mode = probe_plan(f, n);
+  int mode = probe_plan(f, n);
+  if (gather && mode == 1) mode = 2;
   const uint32_t tiles = mode == 1 ? probe_tiles(n_phys) : compact_tiles(n_phys);
   const WsLayout lay = ws_layout(n_phys);
   if (ws_bytes < (mode == 3 ? lay.total : lay.total_small)) return DTLG_ERR_WORKSPACE;
@@ -300,6 +312,14 @@ dtlg_status launch_probe(const dtlg_filter* f, const uint64_t* words, const uint
   c.tile_ctr = a.tile_ctr;
   c.err = a.err;
   c.n_tiles = tiles;
+  if (gather) {
+    c.n_cols = gather->n_cols;
+    for (uint32_t i = 0; i < gather->n_cols; i++) {
+      c.col_bytes[i] = gather->col_bytes[i];
+      c.cols[i] = gather->cols[i];
+      c.out_cols[i] = gather->out_cols[i];
+    }
+  }
   const int cgrid = static_cast<int>(std::min<uint64_t>(tiles, static_cast<uint64_t>(ds->sms) * compact_occupancy()));
   compact_kernel<<<cgrid, kCompactThreads, 0, stream>>>(c);
   DTLG_CUDA(cudaGetLastError());
@@ -499,6 +519,28 @@ dtlg_status dtlg_batch_contains_ws(const dtlg_filter* f, const uint64_t* words, 
   if (dtlg_status st = check_filter_ptr(words)) return st;
   return launch_probe(f, words, keys, n, out, offset, reinterpret_cast<unsigned long long*>(count_dev), ws,
                       ws_bytes, reinterpret_cast<cudaStream_t>(stream));
+}
+
+dtlg_status dtlg_batch_contains_gather(const dtlg_filter* f, const uint64_t* words, const uint32_t* keys,
+                                       uint32_t n, uint32_t n_cols, const void* const* cols,
+                                       const uint32_t* col_bytes, void* const* out_cols, uint32_t* match_positions,
+                                       uint32_t offset, uint64_t* count_dev, void* ws, size_t ws_bytes,
+                                       dtlg_stream_t stream) {
+  if (!f || !count_dev || !ws || (n && !keys)) return DTLG_ERR_NULL;
+  if (n_cols > kMaxGatherCols || (n_cols == 0 && !match_positions)) return DTLG_ERR_INVALID_CONFIG;
+  if (n_cols && (!cols || !col_bytes || !out_cols)) return DTLG_ERR_NULL;
+  GatherSpec g{};
+  g.n_cols = n_cols;
+  for (uint32_t i = 0; i < n_cols; i++) {
+    if (col_bytes[i] != 4 && col_bytes[i] != 8) return DTLG_ERR_INVALID_CONFIG;
+    if (n && (!cols[i] || !out_cols[i])) return DTLG_ERR_NULL;
+    g.col_bytes[i] = col_bytes[i];
+    g.cols[i] = cols[i];
+    g.out_cols[i] = out_cols[i];
+  }
+  if (dtlg_status st = check_filter_ptr(words)) return st;
+  return launch_probe(f, words, keys, n, match_positions, offset, reinterpret_cast<unsigned long long*>(count_dev),
+                      ws, ws_bytes, reinterpret_cast<cudaStream_t>(stream), &g);
 }
 
 dtlg_status dtlg_batch_contains_async(const dtlg_filter* f, const uint64_t* words, const uint32_t* keys,

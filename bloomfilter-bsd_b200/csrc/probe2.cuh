@@ -21,6 +21,7 @@ namespace dtlg {
 constexpr int kCompactThreads = 256;
 constexpr int kCompactWordsPerThread = 8;
 constexpr uint32_t kCompactTileWords = kCompactThreads * kCompactWordsPerThread;
+constexpr uint32_t kMaxGatherCols = 4;
 
 struct CompactArgs {
   const uint32_t* bits;        // key-ordered match bitmask (bit i = physical key i)
@@ -33,6 +34,12 @@ struct CompactArgs {
   unsigned int* tile_ctr;      // zeroed
   unsigned int* err;           // zeroed
   uint32_t n_tiles;
+  // probe -> gather: with every match i (logical index) written to slot j of
+  // the list, row i of each payload column goes to row j of its output column
+  uint32_t n_cols;             // 0 .. kMaxGatherCols
+  uint32_t col_bytes[kMaxGatherCols];  // 4 or 8
+  const void* cols[kMaxGatherCols];
+  void* out_cols[kMaxGatherCols];
 };
 
 #ifdef __CUDACC__
@@ -146,14 +153,23 @@ static __global__ void __launch_bounds__(kCompactThreads) compact_kernel(const _
     }
     __syncthreads();
     uint32_t pos = s_excl + s_warp[warp] + (incl - c);
-    const uint32_t base = static_cast<uint32_t>(w0 * 32 - a.pre) + a.match_offset;
+    const uint32_t first = static_cast<uint32_t>(w0 * 32 - a.pre);  // logical index of bit 0 of wv[0]
 #pragma unroll
     for (int i = 0; i < kCompactWordsPerThread; i++) {
       uint32_t m = wv[i];
       while (m) {
         const uint32_t b = __ffs(m) - 1;
         m &= m - 1;
-        __stcs(a.out + pos, base + static_cast<uint32_t>(i) * 32u + b);
+        const uint32_t li = first + static_cast<uint32_t>(i) * 32u + b;
+        if (a.out) __stcs(a.out + pos, li + a.match_offset);
+        for (uint32_t col = 0; col < a.n_cols; col++) {
+          if (a.col_bytes[col] == 8) {
+            __stcs(static_cast<unsigned long long*>(a.out_cols[col]) + pos,
+                   __ldcs(static_cast<const unsigned long long*>(a.cols[col]) + li));
+          } else {
+            __stcs(static_cast<uint32_t*>(a.out_cols[col]) + pos, __ldcs(static_cast<const uint32_t*>(a.cols[col]) + li));
+          }
+        }
         pos++;
       }
     }

@@ -90,6 +90,8 @@ SIGNATURES = {
     "dtlg_batch_contains_async": (_i, [_vp, _vp, _vp, _u32, _vp, _u32, _vp, _vp]),
     "dtlg_probe_workspace_size": (C.c_size_t, [_u32]),
     "dtlg_batch_contains_ws": (_i, [_vp, _vp, _vp, _u32, _vp, _u32, _vp, _vp, C.c_size_t, _vp]),
+    "dtlg_batch_contains_gather": (_i, [_vp, _vp, _vp, _u32, _u32, _vp, _vp, _vp, _vp, _u32, _vp, _vp, C.c_size_t,
+                                        _vp]),
     "dtlg_batch_contains_noalloc": (_i, [_vp, _vp, _vp, _u32, _vp, _u32, _vp, _vp]),
     "dtlg_set_probe_options": (_i, [_vp, _i, _i]),
     "dtlg_set_probe_passes": (_i, [_vp, _i]),

@@ -188,6 +188,32 @@ class filter_base:  # noqa: N801 (reference name)
                                               int(match_offset) & 0xFFFFFFFF, _dev_ptr(match_cnt_dev, "count"),
                                               _stream()), "batch_contains_async")
 
+    def batch_contains_gather(self, filter_data, keys, cols, out_cols, match_positions=None, match_offset=0):
+        """batch_contains fused with the gather of the matching rows of payload
+        columns (CUDA tensors of 4- or 8-byte elements, one row per key):
+        out_cols[c][j] = cols[c][i] for the j-th match i.  Returns the count."""
+        torch = _torch()
+        keys = as_device_keys(keys, filter_data.device)
+        n = keys.numel()
+        if len(cols) != len(out_cols) or len(cols) > 4:
+            raise ValueError("up to 4 payload columns, one output column each")
+        cp = (C.c_void_p * max(1, len(cols)))(*[_dev_ptr(c, "cols").value for c in cols])
+        op = (C.c_void_p * max(1, len(cols)))(*[_dev_ptr(o, "out_cols").value for o in out_cols])
+        cb = (C.c_uint32 * max(1, len(cols)))(*[c.element_size() for c in cols])
+        for c, o in zip(cols, out_cols):
+            if c.numel() < n or o.numel() < n or c.element_size() != o.element_size():
+                raise ValueError("payload columns need one row per key and outputs of the same type")
+        ws = torch.empty(lib().dtlg_probe_workspace_size(n), dtype=torch.uint8, device=filter_data.device)
+        cnt = torch.zeros(1, dtype=torch.int64, device=filter_data.device)
+        check(lib().dtlg_batch_contains_gather(self._h, _dev_ptr(filter_data, "filter_data"), _dev_ptr(keys, "keys"),
+                                               n, len(cols), cp, cb, op,
+                                               _dev_ptr(match_positions, "match_positions")
+                                               if match_positions is not None else None,
+                                               int(match_offset) & 0xFFFFFFFF, _dev_ptr(cnt, "count"),
+                                               _dev_ptr(ws, "workspace"), ws.numel(), _stream()),
+              "batch_contains_gather")
+        return int(cnt.item())
+
     def batch_contains_host(self, filter_data, keys_host, match_positions_host, match_offset=0):
         """Host key / position buffers (numpy uint32), device filter words."""
         keys_host = np.ascontiguousarray(keys_host, dtype=np.uint32)

@@ -121,6 +121,18 @@ dtlg_status dtlg_batch_contains_ws(const dtlg_filter* f, const uint64_t* filter_
                                    uint32_t match_offset, uint64_t* match_cnt_dev, void* workspace,
                                    size_t workspace_bytes, dtlg_stream_t stream);
 
+/* Probe -> gather, the step after the reference's batch_contains in a
+ * semi-join (the per-tuple work tw of model/cost_fn.hpp:159-166): as
+ * dtlg_batch_contains_ws, and for the match of key i at list slot j also
+ * out_cols[c][j] = cols[c][i] for each of n_cols (<= 4) payload columns of
+ * col_bytes[c] = 4 or 8 bytes (device arrays of n rows / capacity >= n rows).
+ * match_positions may be NULL when n_cols > 0.  Counterpart: none fused; the
+ * reference's callers gather from the position list afterwards. */
+dtlg_status dtlg_batch_contains_gather(const dtlg_filter* f, const uint64_t* filter_words, const uint32_t* keys,
+                                       uint32_t key_cnt, uint32_t n_cols, const void* const* cols,
+                                       const uint32_t* col_bytes, void* const* out_cols, uint32_t* match_positions,
+                                       uint32_t match_offset, uint64_t* match_cnt_dev, void* workspace,
+                                       size_t workspace_bytes, dtlg_stream_t stream);
 /* Probe tuning of one filter (set by the autotuner, dtlg/autotune.py):
  * mode 0 = automatic, 1 = one fused kernel (probe + ordered compaction),
  * 2 = two streaming kernels (match bitmask, then compaction); variant selects
