@@ -504,8 +504,9 @@ def batched_plan(n_filters=512, seed=4242, max_log2=24):
 
 
 def run_batched(args):
-    """512 independent filters built and probed in one
-    persistent, graph-captured launch vs 512 separate per-filter calls."""
+    """512 independent filters (zoned / sectorized, sizes log-uniform up to
+    2^24) built and probed in one persistent, graph-captured launch vs the
+    same work as separate per-filter calls."""
     import ctypes as C
 
     import torch

@@ -1,5 +1,5 @@
 """Configuration choice: the MLP cost model, with the exhaustive search as its
-fallback and judge.
+fallback and as the measure of its error.
 
 The network reads a query -- log2 n, log10 of the FPR target, the probe hit
 ratio, log10 of the downstream work per tuple and the L2-residency flag --
