@@ -60,7 +60,7 @@ struct dtlg_batch {
   std::vector<int> fallback;         // item indexes run as separate launches
   std::vector<void*> fallback_ws;
   std::vector<size_t> fallback_ws_bytes;
-  uint32_t n_menu = 0, n_build_tiles = 0, n_probe_tiles = 0;
+  uint32_t n_menu = 0, n_probe_tiles = 0;
   BatchDesc* d_desc = nullptr;
   char* d_ctl = nullptr;             // ctl words | built counters | status words
   size_t ctl_bytes = 0, built_off = 0, status_off = 0;
@@ -138,7 +138,7 @@ dtlg_status dtlg_batch_prepare(const dtlg_batch_item* items, uint32_t n_items, i
   b->items.assign(items, items + n_items);
   b->use_graph = use_graph != 0;
   std::vector<BatchDesc> desc;
-  uint32_t n_build_tiles = 0, n_probe_tiles = 0;
+  uint32_t n_probe_tiles = 0;
   for (uint32_t i = 0; i < n_items; i++) {
     const dtlg_batch_item& it = items[i];
     if (!it.filter || !it.filter_words || !it.match_cnt || (it.n_build && !it.build_keys) ||
@@ -169,11 +169,9 @@ dtlg_status dtlg_batch_prepare(const dtlg_batch_item* items, uint32_t n_items, i
     d.n_build = it.n_build;
     d.n_probe = it.n_probe;
     d.match_offset = it.match_offset;
-    d.build_tile0 = n_build_tiles;
     d.n_build_tiles = tiles_of(it.n_build);
     d.probe_tile0 = n_probe_tiles;
     d.n_probe_tiles = tiles_of(it.n_probe);
-    n_build_tiles += d.n_build_tiles;
     n_probe_tiles += d.n_probe_tiles;
     const uint32_t f = static_cast<uint32_t>(desc.size());
     desc.push_back(d);
@@ -223,7 +221,6 @@ dtlg_status dtlg_batch_prepare(const dtlg_batch_item* items, uint32_t n_items, i
     b->n_items[v] = static_cast<uint32_t>(queue[v].size());
   }
   b->n_menu = static_cast<uint32_t>(desc.size());
-  b->n_build_tiles = n_build_tiles;
   b->n_probe_tiles = n_probe_tiles;
   b->built_off = 256;
   b->ranges_built_off = b->built_off + round256(static_cast<size_t>(b->n_menu) * 4);

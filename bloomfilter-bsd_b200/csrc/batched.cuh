@@ -54,9 +54,8 @@ struct BatchDesc {
   uint32_t* out;
   unsigned long long* count_out;
   uint32_t n_build, n_probe, match_offset;
-  uint32_t build_tile0, n_build_tiles;  // first global build tile, tile count
-  uint32_t probe_tile0, n_probe_tiles;  // first global probe tile, tile count
-  uint32_t vec32;
+  uint32_t n_build_tiles;               // build tiles of this filter
+  uint32_t probe_tile0, n_probe_tiles;  // first global probe tile (look-back word), tile count
   // staged build (staged != 0): range r holds blocks [r << range_shift, ...)
   uint32_t staged, n_ranges, range_shift, bucket_cap;
   uint32_t* bucket;             // n_ranges x bucket_cap keys
