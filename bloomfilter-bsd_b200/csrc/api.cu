@@ -286,10 +286,24 @@ dtlg_status launch_probe(const dtlg_filter* f, const uint64_t* words, const uint
     pa.totals = reinterpret_cast<uint32_t*>(wsb + lay.totals_off);
     pa.pairs = reinterpret_cast<uint2*>(wsb + lay.pairs_off);
     DTLG_CUDA(cudaMemsetAsync(bits, 0, bits_words(n_phys) * 4, stream));
-    const int pgrid = static_cast<int>(std::min<uint64_t>(pa.n_tiles, static_cast<uint64_t>(ds->sms) * 8));
-    part_hist_kernel<<<pgrid, kPartThreads, 0, stream>>>(pa);
+    // grids of resident CTAs only: the tiles are strided over the grid, so a
+    // second, partial wave would finish its share late (the scatter's 37 KiB
+    // of shared memory allow 6 CTAs per SM, not 8)
+    static const int hist_occ = [] {
+      int o = 0;
+      return cudaOccupancyMaxActiveBlocksPerMultiprocessor(&o, part_hist_kernel, kPartThreads, 0) == cudaSuccess
+                 ? std::max(1, o) : 1;
+    }();
+    static const int scatter_occ = [] {
+      int o = 0;
+      return cudaOccupancyMaxActiveBlocksPerMultiprocessor(&o, part_scatter_kernel, kPartThreads, 0) == cudaSuccess
+                 ? std::max(1, o) : 1;
+    }();
+    const int hgrid = static_cast<int>(std::min<uint64_t>(pa.n_tiles, static_cast<uint64_t>(ds->sms) * hist_occ));
+    const int sgrid = static_cast<int>(std::min<uint64_t>(pa.n_tiles, static_cast<uint64_t>(ds->sms) * scatter_occ));
+    part_hist_kernel<<<hgrid, kPartThreads, 0, stream>>>(pa);
     part_scan_kernel<<<pa.n_ranges, 1024, 0, stream>>>(pa);
-    part_scatter_kernel<<<pgrid, kPartThreads, 0, stream>>>(pa);
+    part_scatter_kernel<<<sgrid, kPartThreads, 0, stream>>>(pa);
     DTLG_CUDA(cudaGetLastError());
     PairsArgs pr{};
     pr.probe = a;
