@@ -26,8 +26,18 @@ static std::vector<CuckooKernels>& cuckoo_table() {
   static std::vector<CuckooKernels> t;
   return t;
 }
+static std::vector<BcfKernels>& bcf_table() {
+  static std::vector<BcfKernels> t;
+  return t;
+}
 void register_bloom(const BloomKernels& k) { bloom_table().push_back(k); }
 void register_cuckoo(const CuckooKernels& k) { cuckoo_table().push_back(k); }
+void register_bcf(const BcfKernels& k) { bcf_table().push_back(k); }
+const BcfKernels* find_bcf(uint32_t t, uint32_t a) {
+  for (const auto& e : bcf_table())
+    if (e.t == t && e.a == a) return &e;
+  return nullptr;
+}
 const BloomKernels* find_bloom(uint32_t wb, uint32_t w, uint32_t s, uint32_t z, uint32_t k) {
   for (const auto& e : bloom_table())
     if (e.word_bytes == wb && e.w == w && e.s == s && e.z == z && e.k == k) return &e;
@@ -168,20 +178,22 @@ dtlg_status check_filter_ptr(const void* p) {
 
 // Probe kernel plan for n keys: 1 = fused (probe + ordered compaction in one
 // kernel), 2 = match bitmask in block-range passes + compaction,
-// 3 = partitioned probe (Bloom filters only) + compaction.
+// 3 = partitioned probe (Bloom and blocked cuckoo filters: one block per key)
+// + compaction.
 // Automatic choice (measured on B200, u64 w=8 s=8 k=8, 2^26-2^28 probes):
 // below 2^20 keys the single fused kernel; Bloom filters above 160 MiB the
 // partitioned probe (256 MiB: 68.6 vs 62.5 Gkeys/s; 512 MiB: 64 vs 54); else
 // the bitmask kernel (L2-resident filters: 113 vs 76 Gkeys/s partitioned).
 int probe_plan(const dtlg_filter* f, uint64_t n) {
   int mode = f->probe_mode;
-  if (mode == 3 && !f->bk) mode = 2;
+  const bool partitioned = f->pk->probe_pairs[0] != nullptr;
+  if (mode == 3 && !partitioned) mode = 2;
   if (mode == 0) {
     const uint64_t bytes = (f->d.m_actual + 7) / 8;
     if (n < kTwoPassMinKeys) {
       mode = 1;
     } else {
-      mode = (f->bk && bytes > (160ull << 20)) ? 3 : 2;
+      mode = (partitioned && bytes > (160ull << 20)) ? 3 : 2;
     }
   }
   return mode;
@@ -243,11 +255,10 @@ dtlg_status launch_probe(const dtlg_filter* f, const uint64_t* words, const uint
   a.tile_ctr = &h->tile_ctr;
   a.err = &h->err;
   a.n_tiles = tiles;
-  a.addr = f->d.addr;
-  a.victim_word = f->d.victim_word;
+  set_filter_args(f->d, &a);
   if (mode == 1) {
-    const probe_fn fn = f->bk ? f->bk->probe : f->ck->probe;
-    const occ_fn occ = f->bk ? f->bk->probe_blocks_per_sm : f->ck->probe_blocks_per_sm;
+    const probe_fn fn = f->pk->probe;
+    const occ_fn occ = f->pk->probe_blocks_per_sm;
     const int per_sm = std::max(1, occ());
     const int grid = static_cast<int>(std::min<uint64_t>(tiles, static_cast<uint64_t>(ds->sms) * per_sm));
     DTLG_CUDA(fn(a, grid, stream));
@@ -260,8 +271,8 @@ dtlg_status launch_probe(const dtlg_filter* f, const uint64_t* words, const uint
     // match bitmask, in block-range passes over large filters (each pass
     // probes only the keys whose block lies in its range, so the concurrently
     // touched part of the filter stays within the GPU's address-translation reach)
-    const probe_bits_fn bfn = f->bk ? f->bk->probe_bits[v] : f->ck->probe_bits[v];
-    const occ_fn bocc = f->bk ? f->bk->bits_blocks_per_sm[v] : f->ck->bits_blocks_per_sm[v];
+    const probe_bits_fn bfn = f->pk->probe_bits[v];
+    const occ_fn bocc = f->pk->bits_blocks_per_sm[v];
     const uint64_t chunks = (n_phys + 127) / 128;  // one warp-chunk = 128 keys
     const uint64_t max_grid = static_cast<uint64_t>(ds->sms) * std::max(1, bocc());
     const int bgrid = static_cast<int>(std::max<uint64_t>(1, std::min<uint64_t>((chunks + 7) / 8, max_grid)));
@@ -280,6 +291,7 @@ dtlg_status launch_probe(const dtlg_filter* f, const uint64_t* words, const uint
     pa.n_phys = n_phys;
     pa.pre = pre;
     pa.addr = f->d.addr;
+    pa.block_mul = mul_const(f->xk ? 1 : 0);
     partition_ranges(f, &pa.range_log2, &pa.n_ranges);
     pa.n_tiles = part_tiles(n_phys);
     pa.counts = reinterpret_cast<uint32_t*>(wsb + lay.counts_off);
@@ -311,8 +323,8 @@ dtlg_status launch_probe(const dtlg_filter* f, const uint64_t* words, const uint
     pr.n_pairs = n;
     pr.bits = bits;
     pr.pre = pre;
-    const int qgrid = static_cast<int>(static_cast<uint64_t>(ds->sms) * std::max(1, f->bk->pairs_blocks_per_sm[v]()));
-    DTLG_CUDA(f->bk->probe_pairs[v](pr, qgrid, stream));
+    const int qgrid = static_cast<int>(static_cast<uint64_t>(ds->sms) * std::max(1, f->pk->pairs_blocks_per_sm[v]()));
+    DTLG_CUDA(f->pk->probe_pairs[v](pr, qgrid, stream));
   }
   // ordered compaction of the bitmask
   CompactArgs c{};
@@ -430,6 +442,7 @@ dtlg_status dtlg_bloom_create(const dtlg_bloom_config* cfg, uint64_t m, dtlg_fil
     delete f;
     return DTLG_ERR_INVALID_CONFIG;
   }
+  f->pk = &f->bk->pk;
   *out = f;
   return DTLG_OK;
 }
@@ -448,6 +461,26 @@ dtlg_status dtlg_cuckoo_create(const dtlg_cuckoo_config* cfg, uint64_t m, dtlg_f
     delete f;
     return DTLG_ERR_INVALID_CONFIG;
   }
+  f->pk = &f->ck->pk;
+  *out = f;
+  return DTLG_OK;
+}
+
+dtlg_status dtlg_blocked_cuckoo_create(const dtlg_blocked_cuckoo_config* cfg, uint64_t m, dtlg_filter** out) {
+  if (!cfg || !out) return DTLG_ERR_NULL;
+  *out = nullptr;
+  dtlg_filter* f = new dtlg_filter();
+  const int rc = describe_bcf(cfg->block_size_bytes, cfg->tag_size_bits, cfg->associativity, m, &f->d);
+  if (rc) {
+    delete f;
+    return rc == 1 ? DTLG_ERR_INVALID_CONFIG : DTLG_ERR_SIZE;
+  }
+  f->xk = find_bcf(f->d.t, f->d.b);
+  if (!f->xk) {
+    delete f;
+    return DTLG_ERR_INVALID_CONFIG;
+  }
+  f->pk = &f->xk->pk;
   *out = f;
   return DTLG_OK;
 }
@@ -484,6 +517,21 @@ dtlg_status dtlg_batch_insert(const dtlg_filter* f, uint64_t* words, const uint3
   DeviceState* ds = nullptr;
   if (dtlg_status st = device_state(&ds)) return st;
   const uint32_t pre = static_cast<uint32_t>((reinterpret_cast<uintptr_t>(keys) & 15u) >> 2);
+  if (f->xk) {
+    // blocked cuckoo: inserts never fail (bcf.cpp:36-40)
+    BcfBuildArgs b{};
+    b.filter = words;
+    b.keys_al = keys - pre;
+    b.n_phys = static_cast<uint64_t>(n) + pre;
+    b.pre = pre;
+    b.addr = f->d.addr;
+    b.bucket_bits = f->d.bucket_bits;
+    b.hash_shift = f->d.hash_shift;
+    static std::atomic<uint64_t> seed_ctr{0x13198A2E03707344ull};
+    b.seed = seed_ctr.fetch_add(0x9E3779B97F4A7C15ull);
+    DTLG_CUDA(f->xk->insert(b, grid_for(b.n_phys, ds->sms), stream));
+    return DTLG_OK;
+  }
   BuildArgs a{};
   a.filter = words;
   a.keys_al = keys - pre;

@@ -37,6 +37,7 @@ constexpr MenuEntry kMenu[] = {{8, 8, 8, 1, 8},   {8, 8, 8, 2, 8}, {8, 8, 8, 4, 
 constexpr auto kBatchedKernel = batched_kernel<Menu0, Menu1, Menu2, Menu3, Menu4, Menu5, Menu6>;
 
 int menu_index(const FilterDesc& d) {
+  if (d.kind != Kind::kBloom && d.kind != Kind::kZoned) return -1;
   for (int i = 0; i < static_cast<int>(sizeof(kMenu) / sizeof(kMenu[0])); i++) {
     const MenuEntry& m = kMenu[i];
     if (m.wb == d.word_bytes && m.w == d.w && m.s == d.s && m.z == d.z && m.k == d.k) return i;

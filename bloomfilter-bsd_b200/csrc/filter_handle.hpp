@@ -9,9 +9,21 @@ struct dtlg_filter {
   dtlg::FilterDesc d;
   const dtlg::BloomKernels* bk = nullptr;
   const dtlg::CuckooKernels* ck = nullptr;
+  const dtlg::BcfKernels* xk = nullptr;   // blocked cuckoo
+  const dtlg::ProbeKernels* pk = nullptr;  // the probe kernels of whichever kind
   // probe tuning (dtlg_set_probe_options): mode 0 = auto, 1 = fused single
   // kernel, 2 = bitmask + compaction; bits_variant -1 = auto
   int probe_mode = 0;
   int bits_variant = -1;
   int probe_passes = 0;  // block-range passes of the two-pass probe; 0 = auto
 };
+
+namespace dtlg {
+// The filter fields of a probe launch.
+inline void set_filter_args(const FilterDesc& d, ProbeArgs* a) {
+  a->addr = d.addr;
+  a->victim_word = d.victim_word;
+  a->bcf_bucket_bits = d.bucket_bits;
+  a->bcf_hash_shift = d.hash_shift;
+}
+}  // namespace dtlg

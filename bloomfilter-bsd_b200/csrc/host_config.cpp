@@ -120,9 +120,51 @@ int describe_cuckoo(uint32_t t, uint32_t b, uint64_t m, FilterDesc* d) {
   return 0;
 }
 
+int describe_bcf(uint32_t block_bytes, uint32_t t, uint32_t a, uint64_t m, FilterDesc* d) {
+  *d = FilterDesc{};
+  // blocked_cuckoofilter.hpp:254-297
+  if (!(block_bytes == 8 || block_bytes == 32 || block_bytes == 64 || block_bytes == 128 || block_bytes == 256 ||
+        block_bytes == 512))
+    return 1;
+  if (!((t == 8 && a == 4) || (t == 8 && a == 8) || (t == 10 && a == 6) || (t == 12 && a == 4) ||
+        (t == 16 && a == 2) || (t == 16 && a == 4)))
+    return 1;
+  d->kind = Kind::kBlockedCuckoo;
+  d->t = t;
+  d->b = a;
+  d->m = m;
+  d->block_bytes = block_bytes;
+  d->word_bytes = t * a <= 32 ? 4 : 8;  // one bucket per word (blocked_cuckoofilter_logic.hpp:280-414)
+  d->w = block_bytes / d->word_bytes;
+  d->bucket_bits = ilog2(d->w);
+  const uint64_t block_bits = block_bytes * 8ull;
+  // blocked_cuckoofilter.hpp:303-312, blocked_cuckoofilter_logic.hpp:59-61
+  const bool magic = !is_pow2(m);
+  const int rc = make_addr((m + block_bits - 1) / block_bits, magic, &d->addr);
+  if (rc) return rc;
+  d->m_actual = static_cast<uint64_t>(d->addr.block_cnt) * block_bits;  // logic.hpp:262-264
+  d->word_cnt = static_cast<uint64_t>(d->addr.block_cnt) * d->w;
+  // the reference forms word indexes in 32 bits (blocked_cuckoofilter_logic.hpp:76)
+  if (d->word_cnt > (1ull << 32)) return 2;
+  // bucket hash: the block hash shifted past the addressing bits when enough
+  // bits remain, else a second hash of the key (logic.hpp:77-82,
+  // block_addressing_logic.hpp:131,230)
+  const uint32_t req = magic ? 32u : ilog2(d->addr.block_cnt);
+  d->hash_shift = req + t + d->bucket_bits <= 32 ? req : 32u;
+  d->size_u64 = d->m_actual / 64;  // block_bytes >= 8: whole 64-bit words
+  d->alloc_u64 = d->size_u64;
+  return 0;
+}
+
 std::string filter_name(const FilterDesc& d) {
   const std::string addr = d.addr.magic_mode ? "\"magic\"" : "\"pow2\"";
   const uint64_t bytes = (d.m_actual + 7) / 8;
+  if (d.kind == Kind::kBlockedCuckoo) {
+    // blocked_cuckoofilter.hpp:445-454
+    return "{\"name\":\"blocked_cuckoo\", \"size\":" + std::to_string(bytes) +
+           ",\"block_size\":" + std::to_string(d.block_bytes) + ",\"tag_bits\":" + std::to_string(d.t) +
+           ",\"associativity\":" + std::to_string(d.b) + ",\"addr\":" + addr + "}";
+  }
   if (d.kind == Kind::kCuckoo) {
     // cuckoofilter.hpp:335-342 ("u" is the SIMD unroll factor of the reference's
     // CPU path; the GPU has none, reported as 0)

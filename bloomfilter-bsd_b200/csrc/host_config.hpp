@@ -1,6 +1,7 @@
 // host_config.hpp -- filter construction rules on the host (validation, sizes,
 // addressing, name).  Reference: blocked_bloomfilter.hpp:96-390,
 // zoned_blocked_bloomfilter.hpp:98-378, cuckoofilter.hpp:115-343,
+// blocked_cuckoofilter.hpp:183-455,
 // block_addressing_logic.hpp:41-235, div.hpp:30-57, filter.hpp:42-72.
 #pragma once
 
@@ -11,7 +12,7 @@
 
 namespace dtlg {
 
-enum class Kind : int { kBloom = 0, kZoned = 1, kCuckoo = 2 };
+enum class Kind : int { kBloom = 0, kZoned = 1, kCuckoo = 2, kBlockedCuckoo = 3 };
 
 // Smallest d >= max(n, 2) whose libdivide u32 magic needs neither the add step
 // nor the power-of-two shift path (div.hpp:30-57; libdivide.h:719-769, the
@@ -26,8 +27,12 @@ struct FilterDesc {
   Kind kind = Kind::kBloom;
   // Bloom
   uint32_t word_bytes = 4, w = 1, s = 1, z = 1, k = 8;
-  // cuckoo
+  // cuckoo (b = tags per bucket) and blocked cuckoo (b = associativity)
   uint32_t t = 16, b = 4, bytes_per_bucket = 8;
+  // blocked cuckoo: block size, log2(buckets per block), bucket-hash shift
+  // (32: the bucket hash is key * C[0]); word_bytes / w hold the bucket word
+  // size and the buckets per block
+  uint32_t block_bytes = 0, bucket_bits = 0, hash_shift = 32;
   uint64_t m = 0, m_actual = 0;
   Addr addr{};
   uint64_t word_cnt = 0;      // Bloom: words of word_bytes; cuckoo: 32-bit table words
@@ -40,6 +45,7 @@ struct FilterDesc {
 int describe_bloom(uint32_t word_size, uint32_t w, uint32_t s, uint32_t z, uint32_t k, uint64_t m,
                    FilterDesc* out);
 int describe_cuckoo(uint32_t t, uint32_t b, uint64_t m, FilterDesc* out);
+int describe_bcf(uint32_t block_bytes, uint32_t t, uint32_t a, uint64_t m, FilterDesc* out);
 std::string filter_name(const FilterDesc& d);
 
 }  // namespace dtlg

@@ -42,12 +42,13 @@ struct PartArgs {
   uint32_t* counts;         // [n_ranges][n_tiles]: counts, then exclusive prefixes
   uint32_t* totals;         // [n_ranges]
   uint2* pairs;             // (key, logical position), grouped by range
+  uint32_t block_mul;       // the family constant of the block hash (C[0]; C[1]: blocked cuckoo)
 };
 
 #ifdef __CUDACC__
 
 __device__ __forceinline__ uint32_t key_range(uint32_t key, const PartArgs& a) {
-  return block_index(key * mul_const(0), a.addr) >> a.range_log2;
+  return block_index(key * a.block_mul, a.addr) >> a.range_log2;
 }
 
 static __global__ void __launch_bounds__(kPartThreads) part_hist_kernel(const __grid_constant__ PartArgs a) {

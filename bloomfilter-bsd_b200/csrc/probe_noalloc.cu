@@ -107,10 +107,9 @@ extern "C" dtlg_status dtlg_batch_contains_noalloc(const dtlg_filter* f, const u
   a.tile_ctr = &h->tile_ctr;
   a.err = &h->err;
   a.n_tiles = tiles;
-  a.addr = f->d.addr;
-  a.victim_word = f->d.victim_word;
-  const probe_fn fn = f->bk ? f->bk->probe : f->ck->probe;
-  const occ_fn occ = f->bk ? f->bk->probe_blocks_per_sm : f->ck->probe_blocks_per_sm;
+  set_filter_args(f->d, &a);
+  const probe_fn fn = f->pk->probe;
+  const occ_fn occ = f->pk->probe_blocks_per_sm;
   const int per_sm = std::max(1, occ());
   const int grid = static_cast<int>(std::min<uint64_t>(tiles, static_cast<uint64_t>(s->sms) * per_sm));
   return fn(a, grid, stream) == cudaSuccess ? DTLG_OK : DTLG_ERR_CUDA;

@@ -5,6 +5,7 @@
 
 #include <cstdint>
 
+#include "bcf.cuh"
 #include "bloom.cuh"
 #include "cuckoo.cuh"
 #include "probe.cuh"
@@ -23,23 +24,25 @@ using probe_bits_fn = cudaError_t (*)(const ProbeArgs&, uint32_t* bits, int or_i
 constexpr int kBitsVariants = 2;
 using pairs_fn = cudaError_t (*)(const PairsArgs&, int grid, cudaStream_t);
 
+// The probe kernels every filter kind provides to the probe plans.
+struct ProbeKernels {
+  probe_fn probe;                               // plan 1: fused probe + compaction
+  occ_fn probe_blocks_per_sm;
+  probe_bits_fn probe_bits[kBitsVariants];      // plan 2: match bitmask
+  occ_fn bits_blocks_per_sm[kBitsVariants];
+  pairs_fn probe_pairs[kBitsVariants];          // plan 3: partitioned (null: not offered)
+  occ_fn pairs_blocks_per_sm[kBitsVariants];
+};
+
 struct BloomKernels {
   uint32_t word_bytes, w, s, z, k;
-  probe_fn probe;
+  ProbeKernels pk;
   build_fn build;
-  occ_fn probe_blocks_per_sm;
-  probe_bits_fn probe_bits[kBitsVariants];
-  occ_fn bits_blocks_per_sm[kBitsVariants];
-  pairs_fn probe_pairs[kBitsVariants];
-  occ_fn pairs_blocks_per_sm[kBitsVariants];
 };
 
 struct CuckooKernels {
   uint32_t t, b;
-  probe_fn probe;
-  occ_fn probe_blocks_per_sm;
-  probe_bits_fn probe_bits[kBitsVariants];
-  occ_fn bits_blocks_per_sm[kBitsVariants];
+  ProbeKernels pk;
   void (*unpack)(const uint32_t* table, uint32_t* slots, uint32_t buckets, int grid, cudaStream_t);
   void (*insert)(const CuckooBuildArgs&, int grid, cudaStream_t);
   void (*pack)(uint32_t* table, const uint32_t* slots, uint32_t buckets, uint64_t words, int grid,
@@ -48,8 +51,16 @@ struct CuckooKernels {
                 int grid, cudaStream_t);
 };
 
+struct BcfKernels {
+  uint32_t t, a;
+  ProbeKernels pk;
+  cudaError_t (*insert)(const BcfBuildArgs&, int grid, cudaStream_t);
+};
+
 void register_bloom(const BloomKernels& k);
 void register_cuckoo(const CuckooKernels& k);
+void register_bcf(const BcfKernels& k);
+const BcfKernels* find_bcf(uint32_t t, uint32_t a);
 const BloomKernels* find_bloom(uint32_t word_bytes, uint32_t w, uint32_t s, uint32_t z, uint32_t k);
 const CuckooKernels* find_cuckoo(uint32_t t, uint32_t b);
 int registered_bloom_count();
@@ -85,50 +96,56 @@ struct PairsLaunch {
   }
 };
 
-template <class Cfg>
-struct BloomLaunch {
-  static cudaError_t probe(const ProbeArgs& a, int grid, cudaStream_t s) {
-    probe_kernel<BloomOps<Cfg>, kProbeRounds><<<grid, kProbeThreads, 0, s>>>(a);
-    return cudaGetLastError();
-  }
-  static cudaError_t build(const BuildArgs& a, int grid, cudaStream_t s) {
-    bloom_build_kernel<Cfg><<<grid, 256, 0, s>>>(a);
+template <class Ops>
+struct FusedLaunch {
+  static cudaError_t run(const ProbeArgs& a, int grid, cudaStream_t s) {
+    probe_kernel<Ops, kProbeRounds><<<grid, kProbeThreads, 0, s>>>(a);
     return cudaGetLastError();
   }
   static int occupancy() {
     int n = 0;
-    cudaOccupancyMaxActiveBlocksPerMultiprocessor(&n, probe_kernel<BloomOps<Cfg>, kProbeRounds>,
-                                                  kProbeThreads, 0);
+    cudaOccupancyMaxActiveBlocksPerMultiprocessor(&n, probe_kernel<Ops, kProbeRounds>, kProbeThreads, 0);
     return n;
   }
 };
 
+template <class Cfg>
+struct BloomLaunch {
+  static cudaError_t build(const BuildArgs& a, int grid, cudaStream_t s) {
+    bloom_build_kernel<Cfg><<<grid, 256, 0, s>>>(a);
+    return cudaGetLastError();
+  }
+};
+
+// Probe kernels of one Ops type; Pairs = false leaves the partitioned plan out.
+template <class Ops, bool Pairs>
+ProbeKernels probe_entry() {
+  using F = FusedLaunch<Ops>;
+  using B8 = BitsLaunch<Ops, 8>;
+  using B4 = BitsLaunch<Ops, 4>;
+  using P8 = PairsLaunch<Ops, 8>;
+  using P4 = PairsLaunch<Ops, 4>;
+  ProbeKernels k{&F::run, &F::occupancy, {&B8::run, &B4::run}, {&B8::occupancy, &B4::occupancy},
+                 {nullptr, nullptr}, {nullptr, nullptr}};
+  if constexpr (Pairs) {
+    k.probe_pairs[0] = &P8::run;
+    k.probe_pairs[1] = &P4::run;
+    k.pairs_blocks_per_sm[0] = &P8::occupancy;
+    k.pairs_blocks_per_sm[1] = &P4::occupancy;
+  }
+  return k;
+}
+
 template <typename Word, int W, int S, int Z, int K>
 BloomKernels bloom_entry() {
   using C = BloomCfg<Word, W, S, Z, K>;
-  using B8 = BitsLaunch<BloomOps<C>, 8>;
-  using B4 = BitsLaunch<BloomOps<C>, 4>;
-  using P8 = PairsLaunch<BloomOps<C>, 8>;
-  using P4 = PairsLaunch<BloomOps<C>, 4>;
-  return BloomKernels{static_cast<uint32_t>(sizeof(Word)), W, S, Z, K, &BloomLaunch<C>::probe,
-                      &BloomLaunch<C>::build, &BloomLaunch<C>::occupancy,
-                      {&B8::run, &B4::run}, {&B8::occupancy, &B4::occupancy},
-                      {&P8::run, &P4::run}, {&P8::occupancy, &P4::occupancy}};
+  return BloomKernels{static_cast<uint32_t>(sizeof(Word)), W, S, Z, K, probe_entry<BloomOps<C>, true>(),
+                      &BloomLaunch<C>::build};
 }
 
 template <int T, int B>
 struct CuckooLaunch {
   using C = CuckooCfg<T, B>;
-  static cudaError_t probe(const ProbeArgs& a, int grid, cudaStream_t s) {
-    probe_kernel<CuckooOps<C>, kProbeRounds><<<grid, kProbeThreads, 0, s>>>(a);
-    return cudaGetLastError();
-  }
-  static int occupancy() {
-    int n = 0;
-    cudaOccupancyMaxActiveBlocksPerMultiprocessor(&n, probe_kernel<CuckooOps<C>, kProbeRounds>,
-                                                  kProbeThreads, 0);
-    return n;
-  }
   static void unpack(const uint32_t* t, uint32_t* sl, uint32_t nb, int grid, cudaStream_t s) {
     cuckoo_unpack_kernel<C><<<grid, 256, 0, s>>>(t, sl, nb);
   }
@@ -144,13 +161,26 @@ struct CuckooLaunch {
   }
 };
 
+// Cuckoo buckets are probed in bucket-range passes, not partitioned: a key's
+// two buckets lie anywhere in the table.
 template <int T, int B>
 CuckooKernels cuckoo_entry() {
   using L = CuckooLaunch<T, B>;
-  using B8 = BitsLaunch<CuckooOps<CuckooCfg<T, B>>, 8>;
-  using B4 = BitsLaunch<CuckooOps<CuckooCfg<T, B>>, 4>;
-  return CuckooKernels{T, B, &L::probe, &L::occupancy, {&B8::run, &B4::run}, {&B8::occupancy, &B4::occupancy},
-                       &L::unpack, &L::insert, &L::pack, &L::count};
+  return CuckooKernels{T, B, probe_entry<CuckooOps<CuckooCfg<T, B>>, false>(), &L::unpack, &L::insert, &L::pack,
+                       &L::count};
+}
+
+template <int T, int A>
+struct BcfLaunch {
+  static cudaError_t insert(const BcfBuildArgs& a, int grid, cudaStream_t s) {
+    bcf_insert_kernel<BcfCfg<T, A>><<<grid, 256, 0, s>>>(a);
+    return cudaGetLastError();
+  }
+};
+
+template <int T, int A>
+BcfKernels bcf_entry() {
+  return BcfKernels{T, A, probe_entry<BcfOps<BcfCfg<T, A>>, true>(), &BcfLaunch<T, A>::insert};
 }
 #endif
 

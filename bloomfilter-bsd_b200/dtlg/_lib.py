@@ -45,6 +45,10 @@ class CuckooConfigS(C.Structure):
     _fields_ = [("bits_per_tag", C.c_uint32), ("tags_per_bucket", C.c_uint32), ("addr_mode", C.c_uint32)]
 
 
+class BcfConfigS(C.Structure):
+    _fields_ = [("block_size_bytes", C.c_uint32), ("tag_size_bits", C.c_uint32), ("associativity", C.c_uint32)]
+
+
 class BatchItemS(C.Structure):
     _fields_ = [("filter", C.c_void_p), ("filter_words", C.c_void_p), ("build_keys", C.c_void_p),
                 ("n_build", C.c_uint32), ("probe_keys", C.c_void_p), ("n_probe", C.c_uint32),
@@ -77,6 +81,7 @@ _u64p = C.POINTER(C.c_uint64)
 SIGNATURES = {
     "dtlg_bloom_create": (_i, [C.POINTER(BloomConfigS), _u64, C.POINTER(_vp)]),
     "dtlg_cuckoo_create": (_i, [C.POINTER(CuckooConfigS), _u64, C.POINTER(_vp)]),
+    "dtlg_blocked_cuckoo_create": (_i, [C.POINTER(BcfConfigS), _u64, C.POINTER(_vp)]),
     "dtlg_destroy": (None, [_vp]),
     "dtlg_size_in_bytes": (_u64, [_vp]),
     "dtlg_size": (_u64, [_vp]),

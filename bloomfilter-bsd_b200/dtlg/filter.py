@@ -113,7 +113,7 @@ class filter_base:  # noqa: N801 (reference name)
         return bool(lib().dtlg_is_magic(self._h))
 
     def kind(self):
-        return ("bloom", "zoned", "cuckoo")[lib().dtlg_kind(self._h)]
+        return ("bloom", "zoned", "cuckoo", "blocked_cuckoo")[lib().dtlg_kind(self._h)]
 
     def set_probe_options(self, mode=0, variant=-1):
         """Probe kernel choice (0 auto, 1 fused, 2 bitmask + compaction) and the
@@ -292,6 +292,22 @@ class cf(filter_base):  # noqa: N801 -- cf.hpp, cf.cpp:18,27
 
     def get_bucket_count(self):
         return self.block_cnt()
+
+
+class bcf(filter_base):  # noqa: N801 -- bcf.hpp:56, bcf.cpp:24-25
+    """The blocked cuckoo filter dtl::bcf: blocks of block_size_bytes, each a
+    small cuckoo table of one-word buckets.  Inserts never fail (bcf.cpp:36-40).
+    Unlike the reference's bcf::size() (32-bit words), size() here counts
+    64-bit words, like every filter_base."""
+
+    def __init__(self, m, block_size_bytes=64, tag_size_bits=16, associativity=4):
+        cfg = _lib.BcfConfigS(block_size_bytes, tag_size_bits, associativity)
+        h = C.c_void_p()
+        check(lib().dtlg_blocked_cuckoo_create(C.byref(cfg), int(m), C.byref(h)),
+              f"blocked cuckoo filter block={block_size_bytes}, t={tag_size_bits}, a={associativity}")
+        super().__init__(h)
+        self.block_size_bytes = block_size_bytes
+        self.tag_size_bits, self.associativity = tag_size_bits, associativity
 
 
 def construct(config, m):

@@ -66,11 +66,29 @@ typedef struct dtlg_cuckoo_config {
   uint32_t addr_mode;       /* informational, as above */
 } dtlg_cuckoo_config;
 
+/* Mirrors the constructor arguments of dtl::bcf, the blocked cuckoo filter
+ * (src/dtl/filter/bcf.hpp:56: block_size_bytes = 64, tag_size_bits = 16,
+ * associativity = 4).  block_size_bytes: 8, 32, 64, 128, 256, 512; (tag bits,
+ * associativity): (8,4) (8,8) (10,6) (12,4) (16,2) (16,4)
+ * (blocked_cuckoofilter.hpp:254-297).  Addressing is POW2 iff m is a power of
+ * two (:303-312). */
+typedef struct dtlg_blocked_cuckoo_config {
+  uint32_t block_size_bytes;
+  uint32_t tag_size_bits;
+  uint32_t associativity;
+} dtlg_blocked_cuckoo_config;
+
 typedef struct dtlg_filter dtlg_filter;
 
 /* ---- construction (filter.hpp:42-72; bbf_32.hpp:53, zbbf_*.hpp, cf.hpp) ---- */
 dtlg_status dtlg_bloom_create(const dtlg_bloom_config* cfg, uint64_t m_bits, dtlg_filter** out);
 dtlg_status dtlg_cuckoo_create(const dtlg_cuckoo_config* cfg, uint64_t m_bits, dtlg_filter** out);
+/* dtl::bcf::bcf(m, block_size_bytes, tag_size_bits, associativity)
+ * (bcf.hpp:56, bcf.cpp:24-25).  dtl::bcf is not a filter_base (bcf.hpp:11):
+ * its size() counts 32-bit words; dtlg_size() here counts 64-bit words (half
+ * of that; blocks are >= 8 bytes) like every other kind. */
+dtlg_status dtlg_blocked_cuckoo_create(const dtlg_blocked_cuckoo_config* cfg, uint64_t m_bits,
+                                       dtlg_filter** out);
 void dtlg_destroy(dtlg_filter* f);
 
 /* ---- sizes and name ---- */
@@ -84,17 +102,19 @@ uint64_t dtlg_size(const dtlg_filter* f);
 uint64_t dtlg_alloc_words_u64(const dtlg_filter* f);
 /* filter_base::name(): the reference's JSON description (filter_base.hpp:48,
  * blocked_bloomfilter.hpp:372-390, zoned_blocked_bloomfilter.hpp:358-378,
- * cuckoofilter.hpp:335-343).  Writes a NUL-terminated string; returns its
+ * cuckoofilter.hpp:335-343, blocked_cuckoofilter.hpp:445-454).  Writes a NUL-terminated string; returns its
  * length (excluding NUL) or the required length if cap is too small. */
 size_t dtlg_name(const dtlg_filter* f, char* buf, size_t cap);
-/* Introspection: 0 = Bloom, 1 = zoned Bloom, 2 = cuckoo; block (bucket) count;
- * 1 if MAGIC addressing. */
+/* Introspection: 0 = Bloom, 1 = zoned Bloom, 2 = cuckoo, 3 = blocked cuckoo;
+ * block (bucket) count; 1 if MAGIC addressing. */
 int dtlg_kind(const dtlg_filter* f);
 uint64_t dtlg_block_cnt(const dtlg_filter* f);
 int dtlg_is_magic(const dtlg_filter* f);
 
 /* ---- build: filter_base::batch_insert (filter_base.hpp:26) ---- */
-/* Bloom: always DTLG_OK on valid input (bbf_32.cpp:41-45).  Cuckoo: returns
+/* Bloom and blocked cuckoo: always DTLG_OK on valid input (bbf_32.cpp:41-45,
+ * bcf.cpp:36-40; a blocked cuckoo key that finds no slot marks its bucket
+ * overflowed, block_logic.hpp:117).  Cuckoo: returns
  * DTLG_ERR_CUCKOO_FULL when some key could not be placed (the reference's
  * `false`, cuckoofilter_logic.hpp:330-337); *failed_out (optional) gets the
  * number of keys lost.  Synchronous w.r.t. `stream` for cuckoo only. */

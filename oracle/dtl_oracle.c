@@ -489,3 +489,178 @@ uint64_t orc_cuckoo_count_occupied(const orc_cuckoo *f, const void *data) {
     for (uint32_t j = 0; j < f->b; j++) cnt += orc_cuckoo_read_tag(f, data, i, j) != 0;
   return cnt + victim(f, data)->used;
 }
+
+/* ======================================================================== */
+/* Blocked cuckoo filter                                                     */
+/* ======================================================================== */
+
+/* blocked_cuckoofilter_multiword_table.hpp:89-110.  Every instantiation the
+ * dispatcher offers (blocked_cuckoofilter.hpp:254-297) holds exactly one
+ * bucket per word, so a block of block_bytes has block_bytes / word_bytes
+ * buckets and bucket i is word i of the block. */
+int orc_bcf_init(orc_bcf *f, uint32_t block_bytes, uint32_t t, uint32_t a, uint64_t m) {
+  memset(f, 0, sizeof(*f));
+  if (!(block_bytes == 8 || block_bytes == 32 || block_bytes == 64 || block_bytes == 128 ||
+        block_bytes == 256 || block_bytes == 512)) return ORC_ERR_CONFIG;
+  if (!((t == 8 && a == 4) || (t == 8 && a == 8) || (t == 10 && a == 6) || (t == 12 && a == 4) ||
+        (t == 16 && a == 2) || (t == 16 && a == 4))) return ORC_ERR_CONFIG;
+  f->block_bytes = block_bytes;
+  f->t = t; f->a = a; f->m = m;
+  f->word_bytes = t * a <= 32 ? 4 : 8;                 /* blocked_cuckoofilter_logic.hpp:280-414 */
+  f->bucket_bits = log2_u64(block_bytes / f->word_bytes);
+  const uint64_t block_bits = (uint64_t)block_bytes * 8;
+  uint32_t mode = is_pow2_u64(m) ? ORC_ADDR_POW2 : ORC_ADDR_MAGIC;  /* blocked_cuckoofilter.hpp:303-312 */
+  int rc = orc_addr_init(&f->addr, (m + block_bits - 1) / block_bits, mode);  /* logic.hpp:59-61 */
+  if (rc) return rc;
+  f->m_actual = (uint64_t)f->addr.block_cnt * block_bits;  /* logic.hpp:262-264 */
+  f->word_cnt = f->m_actual / (8ull * f->word_bytes);
+  /* word indexes are formed in 32 bits (block_idx << log2(words per block),
+   * logic.hpp:76,106): larger filters would wrap */
+  if (f->word_cnt > (1ull << 32)) return ORC_ERR_SIZE;
+  f->size_u32 = (f->m_actual + 31) / 32;                  /* blocked_cuckoofilter.hpp:435-438 */
+  const uint32_t req = mode == ORC_ADDR_MAGIC ? 32u : f->addr.block_cnt_log2;  /* block_addressing_logic.hpp:131,230 */
+  f->hash_shift = req + t + f->bucket_bits <= 32 ? req : 32u;
+  return ORC_OK;
+}
+
+static uint64_t bcf_bucket_mask(const orc_bcf *f) {     /* multiword_table.hpp:100,111 */
+  const uint32_t bits = f->t * f->a;
+  return bits == f->word_bytes * 8 ? ~0ull >> (64 - bits) : (1ull << bits) - 1;
+}
+
+static uint64_t bcf_read(const orc_bcf *f, const void *block, uint32_t i) {   /* :116-123 */
+  return f->word_bytes == 4 ? ((const uint32_t *)block)[i] : ((const uint64_t *)block)[i];
+}
+static void bcf_write(const orc_bcf *f, void *block, uint32_t i, uint64_t v) { /* :127-136 */
+  if (f->word_bytes == 4) ((uint32_t *)block)[i] = (uint32_t)v;
+  else ((uint64_t *)block)[i] = v;
+}
+static uint32_t bcf_tag_at(const orc_bcf *f, uint64_t bucket, uint32_t j) {  /* :146-150 */
+  return (uint32_t)((bucket >> (f->t * j)) & ((1u << f->t) - 1));
+}
+
+/* packed_value<word, t>::contains (blocked_cuckoofilter_util.hpp:14-88): the
+ * SWAR "has a field equal to n" test, with the reference's own field sets.
+ * With 32-bit words and 16-bit tags the reference's constants are 64-bit, so
+ * that test runs in 64 bits on the zero-extended word. */
+static int bcf_has(const orc_bcf *f, uint64_t x, uint32_t n) {
+  uint32_t fields;
+  switch (f->t) {
+    case 8: fields = f->word_bytes * 8 / 8; break;  /* 4 or 8 */
+    case 10: fields = 6; break;
+    case 12: fields = 5; break;
+    default: fields = 4; break;                      /* 16 */
+  }
+  uint64_t L = 0;
+  for (uint32_t i = 0; i < fields; i++) L |= 1ull << (f->t * i);
+  const uint64_t H = L << (f->t - 1);
+  if (f->t == 8 && f->word_bytes == 4) {
+    const uint32_t y = (uint32_t)x ^ (n * (uint32_t)L);
+    return ((y - (uint32_t)L) & ~y & (uint32_t)H) != 0;
+  }
+  const uint64_t y = x ^ ((uint64_t)n * L);
+  return ((y - L) & ~y & H) != 0;
+}
+
+/* Block index, the hash the block's cuckoo table works on, and the block's
+ * base address (blocked_cuckoofilter_logic.hpp:73-82,103-111). */
+static uint32_t bcf_block_hash(const orc_bcf *f, uint32_t key, uint32_t *hv) {
+  const uint32_t h = key * kMul[1];                      /* knuth_32_alt: hash.hpp:73-83 */
+  const uint32_t blk = orc_addr_block(&f->addr, h);
+  *hv = f->hash_shift < 32 ? h << f->hash_shift : key * kMul[0];  /* knuth_32: hash.hpp:59-69 */
+  return blk;
+}
+
+/* blocked_cuckoofilter_block_logic.hpp:45-72,128-133 */
+static uint32_t bcf_bucket(const orc_bcf *f, uint32_t hv) {
+  return f->bucket_bits ? hv >> (32 - f->bucket_bits) : 0u;
+}
+static uint32_t bcf_tag(const orc_bcf *f, uint32_t hv) {
+  uint32_t tag = (hv >> (32 - f->bucket_bits - f->t)) & ((1u << f->t) - 1);
+  return tag + (tag == 0);
+}
+static uint32_t bcf_alt(const orc_bcf *f, uint32_t i, uint32_t tag) {
+  return f->bucket_bits ? i ^ ((tag * ALT_MUL) >> (32 - f->bucket_bits)) : i;
+}
+
+void orc_bcf_locate(const orc_bcf *f, uint32_t key, uint32_t *block, uint32_t *b1, uint32_t *b2,
+                    uint32_t *tag) {
+  uint32_t hv;
+  *block = bcf_block_hash(f, key, &hv);
+  *b1 = bcf_bucket(f, hv);
+  *tag = bcf_tag(f, hv);
+  *b2 = bcf_alt(f, *b1, *tag);
+}
+
+#define BCF_OVERFLOW_TAG 0xFFFFFFFFu   /* multiword_table.hpp:110 */
+#define BCF_RELOCATIONS 10u            /* block_logic.hpp:108 */
+
+/* insert_tag (multiword_table.hpp:203-224) and, with relocate, its kicking
+ * twin insert_tag_relocate (:176-200): the first slot holding the tag or empty
+ * takes it; a full bucket hands back its own tag (insert_tag) or swaps it with
+ * a random slot and hands back the tag it displaced. */
+static uint32_t bcf_insert_tag(const orc_bcf *f, void *block, uint32_t i, uint32_t tag, int relocate,
+                               uint64_t *rng) {
+  uint64_t bucket = bcf_read(f, block, i);
+  if (bucket == bcf_bucket_mask(f)) return BCF_OVERFLOW_TAG;
+  for (uint32_t j = 0; j < f->a; j++) {
+    const uint32_t x = bcf_tag_at(f, bucket, j);
+    if (x == tag) return 0;
+    if (x == 0) {
+      bcf_write(f, block, i, bucket | ((uint64_t)tag << (f->t * j)));
+      return 0;
+    }
+  }
+  if (!relocate) return tag;
+  const uint32_t r = (uint32_t)(xs_next(rng) >> 32) % f->a;
+  const uint32_t old = bcf_tag_at(f, bucket, r);
+  bcf_write(f, block, i, bucket ^ ((uint64_t)(old ^ tag) << (f->t * r)));
+  return old;
+}
+
+/* blocked_cuckoofilter_block_logic.hpp:96-118 */
+static void bcf_block_insert(const orc_bcf *f, void *block, uint32_t i, uint32_t tag, uint64_t *rng) {
+  uint32_t old = bcf_insert_tag(f, block, i, tag, 0, rng);
+  if (old == 0 || old == BCF_OVERFLOW_TAG) return;
+  uint32_t cur = bcf_alt(f, i, tag), curtag = tag;
+  for (uint32_t c = 0; c < BCF_RELOCATIONS; c++) {
+    old = bcf_insert_tag(f, block, cur, curtag, 1, rng);
+    if (old == 0 || old == BCF_OVERFLOW_TAG) return;
+    curtag = old;
+    cur = bcf_alt(f, cur, curtag);
+  }
+  bcf_write(f, block, cur, bcf_bucket_mask(f));   /* mark_overflow: multiword_table.hpp:140-142 */
+}
+
+static void *bcf_block_ptr(const orc_bcf *f, const void *data, uint32_t blk) {
+  return (uint8_t *)data + (uint64_t)blk * f->block_bytes;
+}
+
+void orc_bcf_insert(const orc_bcf *f, void *data, const uint32_t *keys, uint64_t n, uint64_t seed) {
+  uint64_t rng = seed ? seed : 0x9E3779B97F4A7C15ull;
+  for (uint64_t x = 0; x < n; x++) {
+    uint32_t hv;
+    const uint32_t blk = bcf_block_hash(f, keys[x], &hv);
+    bcf_block_insert(f, bcf_block_ptr(f, data, blk), bcf_bucket(f, hv), bcf_tag(f, hv), &rng);
+  }
+}
+
+/* contains_hash (block_logic.hpp:151-158) with find_tag<table, 1>
+ * (multiword_table.hpp:51-67): an overflowed bucket answers every key. */
+int orc_bcf_contains(const orc_bcf *f, const void *data, uint32_t key) {
+  uint32_t blk, i1, i2, tag;
+  orc_bcf_locate(f, key, &blk, &i1, &i2, &tag);
+  const void *block = bcf_block_ptr(f, data, blk);
+  const uint64_t b1 = bcf_read(f, block, i1), b2 = bcf_read(f, block, i2);
+  const uint64_t ovf = bcf_bucket_mask(f);
+  return b1 == ovf || b2 == ovf || bcf_has(f, b1, tag) || bcf_has(f, b2, tag);
+}
+
+/* blocked_cuckoofilter_logic.hpp:120-170 (scalar batch path) */
+uint64_t orc_bcf_batch_contains(const orc_bcf *f, const void *data, const uint32_t *keys,
+                                uint32_t n, uint32_t *match_pos, uint32_t match_offset) {
+  uint64_t cnt = 0;
+  for (uint32_t i = 0; i < n; i++)
+    if (orc_bcf_contains(f, data, keys[i])) match_pos[cnt++] = i + match_offset;
+  return cnt;
+}

@@ -109,6 +109,36 @@ uint64_t orc_cuckoo_count_occupied(const orc_cuckoo *f, const void *data);
 uint32_t orc_cuckoo_read_tag(const orc_cuckoo *f, const void *data, uint64_t i, uint32_t j);
 void orc_cuckoo_index_tag(const orc_cuckoo *f, uint32_t key, uint32_t *i1, uint32_t *i2, uint32_t *tag);
 
+/* ---------------------------------------------------------------------------
+ * Blocked cuckoo filter (blocked_cuckoofilter/blocked_cuckoofilter*.hpp,
+ * wrapped as dtl::bcf in bcf.hpp:11-63).  Each block is a small cuckoo table
+ * of one-word buckets; a key touches only its own block.
+ * ------------------------------------------------------------------------- */
+typedef struct {
+  uint32_t block_bytes;     /* 8, 32, 64, 128, 256 or 512 */
+  uint32_t t, a;            /* bits per tag, tags per bucket (associativity) */
+  uint32_t word_bytes;      /* one bucket = one word: 4 if t*a <= 32, else 8 */
+  uint32_t bucket_bits;     /* log2(buckets per block) */
+  uint32_t hash_shift;      /* POW2 with log2(B) + t + bucket_bits <= 32: log2(B)
+                               (bucket hash = block hash << log2(B)); else 32:
+                               the bucket hash is key * C[0] */
+  orc_addr addr;
+  uint64_t m, m_actual;
+  uint64_t word_cnt;        /* words of word_bytes */
+  uint64_t size_u32;        /* blocked_cuckoofilter::size(): 32-bit words */
+} orc_bcf;
+
+int orc_bcf_init(orc_bcf *f, uint32_t block_bytes, uint32_t t, uint32_t a, uint64_t m);
+/* Sequential insert (blocked_cuckoofilter_logic.hpp:73-95); kick slots from a
+ * seeded xorshift generator in place of the reference's thread-local mt19937. */
+void orc_bcf_insert(const orc_bcf *f, void *data, const uint32_t *keys, uint64_t n, uint64_t seed);
+int orc_bcf_contains(const orc_bcf *f, const void *data, uint32_t key);
+uint64_t orc_bcf_batch_contains(const orc_bcf *f, const void *data, const uint32_t *keys,
+                                uint32_t n, uint32_t *match_pos, uint32_t match_offset);
+/* Block, both bucket indexes and the tag of a key. */
+void orc_bcf_locate(const orc_bcf *f, uint32_t key, uint32_t *block, uint32_t *b1, uint32_t *b2,
+                    uint32_t *tag);
+
 /* Parallel (pthreads) batch_contains over contiguous slices; used only as the
  * timed CPU baseline.  Returns the total match count; per-slice positions are
  * written to match_pos[slice_begin ...] (not compacted). */

@@ -3,9 +3,11 @@
 TEST INFRASTRUCTURE ONLY: imported by tests/, by __graft_entry__.smoke() and by
 bench.py's CPU-baseline / reference legs, never by the product package.
 
-* ``Bloom`` / ``Cuckoo`` wrap liboracle.so, the C restatement (dtl_oracle.c).
+* ``Bloom`` / ``Cuckoo`` / ``BlockedCuckoo`` wrap liboracle.so, the C
+  restatement (dtl_oracle.c).
 * ``RefLib`` wraps oracle/_ref/libdtlref_*.so, the reference's own filter logic
   compiled from its sources (see oracle/Makefile); absent when not built.
+  ``RefBcf`` wraps oracle/_ref/libdtlref_bcf*.so, the reference's dtl::bcf.
 """
 import ctypes as C
 import os
@@ -31,6 +33,12 @@ class _CuckooS(C.Structure):
     _fields_ = [("t", C.c_uint32), ("b", C.c_uint32), ("bytes_per_bucket", C.c_uint32), ("addr", _Addr),
                 ("m", C.c_uint64), ("m_actual", C.c_uint64), ("table_words_u32", C.c_uint64),
                 ("size_u64", C.c_uint64), ("alloc_u64", C.c_uint64)]
+
+
+class _BcfS(C.Structure):
+    _fields_ = [("block_bytes", C.c_uint32), ("t", C.c_uint32), ("a", C.c_uint32), ("word_bytes", C.c_uint32),
+                ("bucket_bits", C.c_uint32), ("hash_shift", C.c_uint32), ("addr", _Addr), ("m", C.c_uint64),
+                ("m_actual", C.c_uint64), ("word_cnt", C.c_uint64), ("size_u32", C.c_uint64)]
 
 
 _lib = None
@@ -75,6 +83,14 @@ def lib():
         L.orc_cuckoo_read_tag.restype = C.c_uint32
         L.orc_cuckoo_read_tag.argtypes = [C.POINTER(_CuckooS), C.c_void_p, C.c_uint64, C.c_uint32]
         L.orc_cuckoo_index_tag.argtypes = [C.POINTER(_CuckooS), C.c_uint32] + [C.POINTER(C.c_uint32)] * 3
+        L.orc_bcf_init.restype = C.c_int
+        L.orc_bcf_init.argtypes = [C.POINTER(_BcfS)] + [C.c_uint32] * 3 + [C.c_uint64]
+        L.orc_bcf_insert.argtypes = [C.POINTER(_BcfS), C.c_void_p, _u32p, C.c_uint64, C.c_uint64]
+        L.orc_bcf_contains.restype = C.c_int
+        L.orc_bcf_contains.argtypes = [C.POINTER(_BcfS), C.c_void_p, C.c_uint32]
+        L.orc_bcf_batch_contains.restype = C.c_uint64
+        L.orc_bcf_batch_contains.argtypes = [C.POINTER(_BcfS), C.c_void_p, _u32p, C.c_uint32, _u32p, C.c_uint32]
+        L.orc_bcf_locate.argtypes = [C.POINTER(_BcfS), C.c_uint32] + [C.POINTER(C.c_uint32)] * 4
         _lib = L
     return _lib
 
@@ -200,6 +216,66 @@ class Cuckoo:
         return a.value, b.value, t.value
 
 
+class BlockedCuckoo:
+    """C restatement of one blocked cuckoo filter config (data owned by caller)."""
+
+    def __init__(self, m, block_bytes=64, t=16, a=4):
+        self.s_ = _BcfS()
+        rc = lib().orc_bcf_init(C.byref(self.s_), block_bytes, t, a, m)
+        if rc:
+            raise ValueError(f"invalid blocked cuckoo config rc={rc}")
+
+    @property
+    def size_u32(self):
+        return self.s_.size_u32
+
+    @property
+    def size_u64(self):
+        return (self.s_.size_u32 + 1) // 2
+
+    @property
+    def m_actual(self):
+        return self.s_.m_actual
+
+    @property
+    def block_cnt(self):
+        return self.s_.addr.block_cnt
+
+    @property
+    def magic(self):
+        return self.s_.addr.mode == 1
+
+    @property
+    def word_bytes(self):
+        return self.s_.word_bytes
+
+    @property
+    def hash_shift(self):
+        return self.s_.hash_shift
+
+    def alloc(self):
+        return np.zeros(max(1, self.size_u64), dtype=np.uint64)
+
+    def insert(self, data, keys, seed=1):
+        k = _keys(keys)
+        lib().orc_bcf_insert(C.byref(self.s_), data.ctypes.data, k, len(k), seed)
+
+    def contains(self, data, key):
+        return bool(lib().orc_bcf_contains(C.byref(self.s_), data.ctypes.data, int(key)))
+
+    def batch_contains(self, data, keys, match_offset=0):
+        k = _keys(keys)
+        out = np.zeros(max(1, len(k)), dtype=np.uint32)
+        n = lib().orc_bcf_batch_contains(C.byref(self.s_), data.ctypes.data, k, len(k), out,
+                                         match_offset & 0xFFFFFFFF)
+        return out[:n].copy()
+
+    def locate(self, key):
+        r = [C.c_uint32() for _ in range(4)]
+        lib().orc_bcf_locate(C.byref(self.s_), int(key), *[C.byref(x) for x in r])
+        return tuple(x.value for x in r)  # block, bucket 1, bucket 2, tag
+
+
 # --------------------------------------------------------------------------
 # The reference compiled from its sources (oracle/_ref)
 # --------------------------------------------------------------------------
@@ -320,5 +396,96 @@ class _RefFilter:
 def try_reflib():
     try:
         return RefLib()
+    except (FileNotFoundError, OSError):
+        return None
+
+
+class RefBcf:
+    """The reference's dtl::bcf (oracle/_ref/libdtlref_bcf.so: plain x86-64,
+    the scalar batch path; variant "avx2": the AVX2 batch path)."""
+
+    def __init__(self, variant="scalar"):
+        name = "libdtlref_bcf.so" if variant == "scalar" else f"libdtlref_bcf_{variant}.so"
+        path = os.path.join(HERE, "_ref", name)
+        if not os.path.exists(path):
+            raise FileNotFoundError(path)
+        self.variant, self.path = variant, path
+        L = C.CDLL(path)
+        vp = C.c_void_p
+        L.ref_bcf_create.restype = vp
+        L.ref_bcf_create.argtypes = [C.c_uint64, C.c_uint32, C.c_uint32, C.c_uint32]
+        L.ref_bcf_destroy.argtypes = [vp]
+        L.ref_bcf_size.restype = C.c_uint64
+        L.ref_bcf_size.argtypes = [vp]
+        L.ref_bcf_size_in_bytes.restype = C.c_uint64
+        L.ref_bcf_size_in_bytes.argtypes = [vp]
+        L.ref_bcf_name.restype = C.c_size_t
+        L.ref_bcf_name.argtypes = [vp, C.c_char_p, C.c_size_t]
+        L.ref_bcf_batch_insert.restype = C.c_int
+        L.ref_bcf_batch_insert.argtypes = [vp, vp, _u32p, C.c_uint32]
+        L.ref_bcf_contains.restype = C.c_int
+        L.ref_bcf_contains.argtypes = [vp, vp, C.c_uint32]
+        L.ref_bcf_batch_contains.restype = C.c_uint64
+        L.ref_bcf_batch_contains.argtypes = [vp, vp, _u32p, C.c_uint32, _u32p, C.c_uint32]
+        L.ref_bcf_batch_contains_mt.restype = C.c_uint64
+        L.ref_bcf_batch_contains_mt.argtypes = [vp, vp, _u32p, C.c_uint64, _u32p, C.c_int]
+        self.L = L
+
+    def create(self, m, block_bytes=64, t=16, a=4):
+        h = self.L.ref_bcf_create(m, block_bytes, t, a)
+        return _RefBcfFilter(self, h) if h else None
+
+
+class _RefBcfFilter:
+    def __init__(self, ref, h):
+        self.ref, self.h = ref, h
+
+    def __del__(self):
+        try:
+            self.ref.L.ref_bcf_destroy(self.h)
+        except Exception:
+            pass
+
+    @property
+    def size_u32(self):
+        return self.ref.L.ref_bcf_size(self.h)
+
+    @property
+    def size_in_bytes(self):
+        return self.ref.L.ref_bcf_size_in_bytes(self.h)
+
+    def name(self):
+        buf = C.create_string_buffer(512)
+        self.ref.L.ref_bcf_name(self.h, buf, 512)
+        return buf.value.decode()
+
+    def alloc(self):
+        # the reference's words, plus 64 bytes of slack for the AVX2 path's
+        # 256-bit stores past the last match
+        return np.zeros(self.size_u32 + 16, dtype=np.uint32)
+
+    def insert(self, data, keys):
+        k = _keys(keys)
+        return bool(self.ref.L.ref_bcf_batch_insert(self.h, data.ctypes.data, k, len(k)))
+
+    def contains(self, data, key):
+        return bool(self.ref.L.ref_bcf_contains(self.h, data.ctypes.data, int(key)))
+
+    def batch_contains(self, data, keys, match_offset=0):
+        k = _keys(keys)
+        out = np.zeros(len(k) + 16, dtype=np.uint32)
+        n = self.ref.L.ref_bcf_batch_contains(self.h, data.ctypes.data, k, len(k), out, match_offset & 0xFFFFFFFF)
+        return out[:n].copy()
+
+    def batch_contains_mt(self, data, keys, threads, out=None):
+        k = _keys(keys)
+        if out is None:
+            out = np.zeros(len(k) + 16, dtype=np.uint32)
+        return self.ref.L.ref_bcf_batch_contains_mt(self.h, data.ctypes.data, k, len(k), out, threads)
+
+
+def try_refbcf(variant="scalar"):
+    try:
+        return RefBcf(variant)
     except (FileNotFoundError, OSError):
         return None
