@@ -42,6 +42,12 @@ CUCKOO_WORKLOADS = {
     # name: (bits per tag, tags per bucket, log2 n, load factor, log2 probes, hit ratio)
     "cuckoo_dram": (16, 4, 26, 0.95, 28, 0.10),
 }
+BCF_WORKLOADS = {
+    # name: (block bytes, tag bits, associativity, log2 n, log2 m bits, log2 probes, hit ratio)
+    # dtl::bcf's default config: 64-byte blocks of 8 buckets x 4 16-bit tags,
+    # 256 MiB (DRAM-resident) at half of its slots
+    "bcf_dram": (64, 16, 4, 26, 31, 28, 0.10),
+}
 SEED = 20240601
 
 
@@ -51,7 +57,8 @@ def parse():
     ap.add_argument("--steps", type=int, default=100)
     ap.add_argument("--warmup", type=int, default=5)
     ap.add_argument("--impl", choices=("dtlg", "reference"), default="dtlg")
-    ap.add_argument("--workload", choices=sorted(WORKLOADS) + sorted(CUCKOO_WORKLOADS) + ["batched512"],
+    ap.add_argument("--workload", choices=sorted(WORKLOADS) + sorted(CUCKOO_WORKLOADS) + sorted(BCF_WORKLOADS)
+                    + ["batched512"],
                     default="sectorized_dram")
     ap.add_argument("--no-cpu-baseline", action="store_true")
     ap.add_argument("--batch-filters", type=int, default=512, help="batched512: number of filters")
@@ -77,7 +84,27 @@ def cuckoo_bits(n, t, b, lf):
     raise RuntimeError("no odd MAGIC bucket count found")
 
 
+def bcf_sectors(block_bytes, t, a):
+    """Distinct 32-byte sectors a blocked cuckoo probe reads: its two bucket
+    words lie in one block; x = i1 ^ i2 is uniform over the block's buckets,
+    and both words share a sector iff x < buckets per sector."""
+    word = 4 if t * a <= 32 else 8
+    per_block = block_bytes // word
+    if block_bytes <= 32:
+        return 1.0
+    return 2.0 - (32 // word) / per_block
+
+
 def workload_config(name, n_gpus):
+    if name in BCF_WORKLOADS:
+        bb, t, a, ln, lm, lp, h = BCF_WORKLOADS[name]
+        return {
+            "workload": name, "filter": f"blocked cuckoo (dtl::bcf) block={bb} B t={t} a={a}",
+            "build_keys": 1 << ln, "probe_keys_per_gpu": 1 << lp, "global_batch": (1 << lp) * n_gpus,
+            "hit_ratio": h, "filter_bytes": (1 << lm) // 8,
+            "parallelism": f"dp{n_gpus} (replicated filter, sharded probes)",
+            "l2_flush": "inputs larger than L2 (keys 4 B/key x probes + filter words)",
+        }
     if name in CUCKOO_WORKLOADS:
         t, b, ln, lf, lp, h = CUCKOO_WORKLOADS[name]
         return {
@@ -179,20 +206,30 @@ def cpu_reference_probe(words_np, cfg, m, probe_np, threads, budget_s, want_kind
     import numpy as np
 
     import oracle as O
-    ref = O.try_reflib() if want_kind == "reference" else None
     out = np.empty(len(probe_np) + 64, dtype=np.uint32)
-    f = None
-    if ref is not None:
-        f = ref.cuckoo(cfg[1], cfg[2], m) if cfg[0] == "cuckoo" else ref.bloom(*cfg, m)
-    if f is not None:
+    if cfg[0] == "bcf":
+        ref = bcf_reference() if want_kind == "reference" else None
+        if ref is None:
+            raise RuntimeError("the reference's dtl::bcf is not built (oracle/_ref)")
+        f = ref.create(m, cfg[1], cfg[2], cfg[3])
+        words_u32 = np.zeros(f.size_u32 + 16, dtype=np.uint32)
+        words_u32[: f.size_u32] = words_np.view(np.uint32)[: f.size_u32]
         kind = "reference"
-        run = lambda keys: f.batch_contains_mt(words_np, keys, threads, unroll=1, out=out)  # noqa: E731
+        run = lambda keys: f.batch_contains_mt(words_u32, keys, threads, out=out)  # noqa: E731
     else:
-        if cfg[0] == "cuckoo":
-            raise RuntimeError("the reference build lacks this cuckoo config")
-        f = O.Bloom(*cfg, m)
-        kind = "port"
-        run = lambda keys: f.batch_contains_mt(words_np, keys, threads)  # noqa: E731
+        ref = O.try_reflib() if want_kind == "reference" else None
+        f = None
+        if ref is not None:
+            f = ref.cuckoo(cfg[1], cfg[2], m) if cfg[0] == "cuckoo" else ref.bloom(*cfg, m)
+        if f is not None:
+            kind = "reference"
+            run = lambda keys: f.batch_contains_mt(words_np, keys, threads, unroll=1, out=out)  # noqa: E731
+        else:
+            if cfg[0] == "cuckoo":
+                raise RuntimeError("the reference build lacks this cuckoo config")
+            f = O.Bloom(*cfg, m)
+            kind = "port"
+            run = lambda keys: f.batch_contains_mt(words_np, keys, threads)  # noqa: E731
     # size the sample so one pass takes about budget_s
     n = min(len(probe_np), 1 << 20)
     t0 = time.perf_counter()
@@ -207,6 +244,18 @@ def cpu_reference_probe(words_np, cfg, m, probe_np, threads, budget_s, want_kind
         dt = time.perf_counter() - t0
         best = dt if best is None else min(best, dt)
     return n / best, kind, n, cnt, (ref.variant if kind == "reference" else "c")
+
+
+def bcf_reference():
+    """The reference's dtl::bcf (oracle/_ref): its AVX2 build where the host
+    has AVX2 (the build a user compiling for this host runs), else scalar."""
+    sys.path.insert(0, os.path.join(ROOT, "oracle"))
+    import oracle as O
+    if "avx2" in O._cpu_flags():
+        r = O.try_refbcf("avx2")
+        if r is not None:
+            return r
+    return O.try_refbcf("scalar")
 
 
 # ---------------------------------------------------------------------------
@@ -232,6 +281,12 @@ def run_dtlg(args):
         m = cuckoo_bits(n_build, tag_bits, slots, lf)
         f = dtlg.cf(m, tag_bits, slots)
         block_bytes, sectors = (tag_bits * slots + 7) // 8, 2   # two buckets, 8-byte aligned: one sector each
+    elif args.workload in BCF_WORKLOADS:
+        block_bytes, tag_bits, assoc, ln, lm, lp, hit = BCF_WORKLOADS[args.workload]
+        n_build, P = 1 << ln, 1 << lp
+        m = 1 << lm
+        f = dtlg.bcf(m, block_bytes, tag_bits, assoc)
+        sectors = bcf_sectors(block_bytes, tag_bits, assoc)
     else:
         wb, w, s, z, k, ln, bpk, lp, hit = WORKLOADS[args.workload]
         n_build, P = 1 << ln, 1 << lp
@@ -378,7 +433,12 @@ def run_dtlg(args):
             threads = len(os.sched_getaffinity(0))
             words_np = words.cpu().numpy().view(np.uint64)
             probe_np = keys.cpu().numpy().view(np.uint32)
-            fcfg = ("cuckoo", tag_bits, slots) if args.workload in CUCKOO_WORKLOADS else (wb, w, s, z, k)
+            if args.workload in CUCKOO_WORKLOADS:
+                fcfg = ("cuckoo", tag_bits, slots)
+            elif args.workload in BCF_WORKLOADS:
+                fcfg = ("bcf", block_bytes, tag_bits, assoc)
+            else:
+                fcfg = (wb, w, s, z, k)
             rate, kind, n, c, variant = cpu_reference_probe(words_np, fcfg, m, probe_np, threads, budget_s=4.0)
             result["cpu_baseline"] = {"value": round(rate / 1e9, 4), "unit": "Gkeys/s", "cores": threads,
                                       "kind": kind,
@@ -422,6 +482,9 @@ def run_reference(args):
         return
     threads = len(os.sched_getaffinity(0))
     chunk = 1 << 24
+    if args.workload in BCF_WORKLOADS:
+        run_reference_bcf(args, threads, chunk)
+        return
     if args.workload in CUCKOO_WORKLOADS:
         t, b, ln, lf, lp, hit = CUCKOO_WORKLOADS[args.workload]
         n_build, P = 1 << ln, 1 << lp
@@ -479,6 +542,56 @@ def run_reference(args):
                          "sample": f"{n} of the workload's probe keys per step, {threads} threads x 1024-key "
                                    f"batches (model/benchmark.cpp:123-165), SIMD batch_contains "
                                    f"({ref.variant}, {ref.lanes} lanes)", "match_count": int(cnt)},
+        "e2e": {"value": round(value, 4), "unit": "Gkeys/s", "h2d_bytes_per_step": 0, "d2h_bytes_per_step": 0},
+    }), flush=True)
+
+
+def run_reference_bcf(args, threads, chunk):
+    """--impl reference for the blocked cuckoo workloads: the reference's
+    dtl::bcf (bcf.cpp compiled from its sources), built by one thread (its
+    inserts are not atomic), probed by all host threads."""
+    import numpy as np
+
+    from dtlg import keygen
+    world = int(os.environ.get("WORLD_SIZE", "1"))
+    ref = bcf_reference()
+    if ref is None:
+        print(json.dumps({"impl": "reference", "unavailable": "oracle/_ref/libdtlref_bcf*.so (the reference's "
+                                                               "dtl::bcf) is not built on this machine"}))
+        return
+    bb, t, a, ln, lm, lp, hit = BCF_WORKLOADS[args.workload]
+    n_build, P = 1 << ln, 1 << lp
+    f = ref.create(1 << lm, bb, t, a)
+    words = f.alloc()
+    for c0 in range(0, n_build, chunk):
+        f.insert(words, keygen.build_keys(min(chunk, n_build - c0), SEED, start=c0))
+    probe = np.concatenate([keygen.probe_keys(n_build, min(chunk, P - c0), hit, SEED, start=c0)[0]
+                            for c0 in range(0, min(P, 1 << 26), chunk)])
+    out = np.empty(len(probe) + 64, dtype=np.uint32)
+    t0 = time.perf_counter()
+    f.batch_contains_mt(words, probe[:1 << 22], threads, out=out)
+    rate0 = (1 << 22) / max(1e-6, time.perf_counter() - t0)
+    n = int(min(len(probe), max(1 << 22, rate0 * 2.0)))
+    for _ in range(max(1, args.warmup)):
+        f.batch_contains_mt(words, probe[:n], threads, out=out)
+    times = []
+    cnt = 0
+    for _ in range(args.steps):
+        t0 = time.perf_counter()
+        cnt = f.batch_contains_mt(words, probe[:n], threads, out=out)
+        times.append(time.perf_counter() - t0)
+    ms = 1e3 * statistics.mean(times)
+    value = n / (ms / 1e3) / 1e9
+    print(json.dumps({
+        "impl": "reference", "metric": "probe Gkeys/s (batch_contains, ascending match positions)",
+        "value": round(value, 4), "unit": "Gkeys/s", "n_gpus": world, "steps": args.steps,
+        "warmup": args.warmup, "ms_per_step": round(ms, 3), "higher_is_better": True, "scaling": "weak",
+        "vs_baseline": None, "dtype": "u32", "data": "synthetic: seeded u32 bijection keys",
+        "config": workload_config(args.workload, world),
+        "cpu_baseline": {"value": round(value, 4), "unit": "Gkeys/s", "cores": threads, "kind": "reference",
+                         "sample": f"{n} of the workload's probe keys per step, {threads} threads x 1024-key "
+                                   f"batches (model/benchmark.cpp:123-165), dtl::bcf batch_contains "
+                                   f"({ref.variant} build)", "match_count": int(cnt)},
         "e2e": {"value": round(value, 4), "unit": "Gkeys/s", "h2d_bytes_per_step": 0, "d2h_bytes_per_step": 0},
     }), flush=True)
 

@@ -33,6 +33,12 @@ static std::vector<BcfKernels>& bcf_table() {
 void register_bloom(const BloomKernels& k) { bloom_table().push_back(k); }
 void register_cuckoo(const CuckooKernels& k) { cuckoo_table().push_back(k); }
 void register_bcf(const BcfKernels& k) { bcf_table().push_back(k); }
+static std::vector<ClassicKernels>& classic_table() {
+  static std::vector<ClassicKernels> t;
+  return t;
+}
+void register_classic(const ClassicKernels& k) { classic_table().push_back(k); }
+const ClassicKernels* find_classic() { return classic_table().empty() ? nullptr : &classic_table()[0]; }
 const BcfKernels* find_bcf(uint32_t t, uint32_t a) {
   for (const auto& e : bcf_table())
     if (e.t == t && e.a == a) return &e;
@@ -154,6 +160,9 @@ int compact_occupancy() {
 // filters are probed in passes of about 256 MiB each; filters up to 160 MiB
 // take one pass.  dtlg_set_probe_passes overrides the choice.
 uint32_t probe_passes(const dtlg_filter* f) {
+  // a classic Bloom key's k words lie anywhere in the filter, and a key
+  // matches only if all are set: its probe cannot be split by word range
+  if (f->qk) return 1;
   const uint64_t bytes = (f->d.m_actual + 7) / 8;
   uint64_t r = f->probe_passes;
   if (r == 0 && f->ck) {
@@ -466,6 +475,26 @@ dtlg_status dtlg_cuckoo_create(const dtlg_cuckoo_config* cfg, uint64_t m, dtlg_f
   return DTLG_OK;
 }
 
+dtlg_status dtlg_classic_bloom_create(const dtlg_classic_bloom_config* cfg, uint64_t m, dtlg_filter** out) {
+  if (!cfg || !out) return DTLG_ERR_NULL;
+  *out = nullptr;
+  if (cfg->addr_mode > 1) return DTLG_ERR_INVALID_CONFIG;
+  dtlg_filter* f = new dtlg_filter();
+  const int rc = describe_classic(cfg->k, m, cfg->addr_mode == 1, &f->d);
+  if (rc) {
+    delete f;
+    return rc == 1 ? DTLG_ERR_INVALID_CONFIG : DTLG_ERR_SIZE;
+  }
+  f->qk = find_classic();
+  if (!f->qk) {
+    delete f;
+    return DTLG_ERR_INVALID_CONFIG;
+  }
+  f->pk = &f->qk->pk;
+  *out = f;
+  return DTLG_OK;
+}
+
 dtlg_status dtlg_blocked_cuckoo_create(const dtlg_blocked_cuckoo_config* cfg, uint64_t m, dtlg_filter** out) {
   if (!cfg || !out) return DTLG_ERR_NULL;
   *out = nullptr;
@@ -517,6 +546,19 @@ dtlg_status dtlg_batch_insert(const dtlg_filter* f, uint64_t* words, const uint3
   DeviceState* ds = nullptr;
   if (dtlg_status st = device_state(&ds)) return st;
   const uint32_t pre = static_cast<uint32_t>((reinterpret_cast<uintptr_t>(keys) & 15u) >> 2);
+  if (f->qk) {
+    ClassicBuildArgs c{};
+    c.filter = reinterpret_cast<uint32_t*>(words);
+    c.keys_al = keys - pre;
+    c.n_phys = static_cast<uint64_t>(n) + pre;
+    c.pre = pre;
+    c.addr = f->d.addr;
+    c.k = f->d.k;
+    c.bit_shift = f->d.bit_shift;
+    c.bit_mask = f->d.bit_mask;
+    DTLG_CUDA(f->qk->build(c, grid_for(c.n_phys, ds->sms), stream));
+    return DTLG_OK;
+  }
   if (f->xk) {
     // blocked cuckoo: inserts never fail (bcf.cpp:36-40)
     BcfBuildArgs b{};

@@ -32,6 +32,7 @@
 #include <cstdint>
 #include <type_traits>
 
+#include "bloom.cuh"
 #include "common.cuh"
 #include "probe.cuh"
 
@@ -117,6 +118,39 @@ struct BcfOps {
     return i ^ static_cast<uint32_t>(static_cast<unsigned long long>(tag * kBcfAltMul) >> (32u - bb));
   }
 
+  // Word j (< words per 32-byte sector) of a sector held as four u64.
+  __device__ __forceinline__ static Word pick(const unsigned long long (&v)[4], uint32_t j) {
+    if constexpr (Cfg::kWide) {
+      return j == 0 ? v[0] : (j == 1 ? v[1] : (j == 2 ? v[2] : v[3]));
+    } else {
+      const unsigned long long x = (j >> 1) == 0 ? v[0] : ((j >> 1) == 1 ? v[1] : ((j >> 1) == 2 ? v[2] : v[3]));
+      return static_cast<Word>(x >> (32u * (j & 1u)));
+    }
+  }
+
+  // The two bucket words of a block.  Every load of a random address costs an
+  // L1 lookup of its own, so blocks of >= 32 bytes on a 32-byte aligned filter
+  // read the 32-byte sector of the first bucket with one 256-bit load and
+  // fetch the second word separately only when it lies in another sector
+  // (half the keys in a 64-byte block); a one-word block is read once.
+  __device__ __forceinline__ static void load_pair(const Word* p, uint32_t i1, uint32_t i2, uint32_t bb,
+                                                   bool vec32, Word& w1, Word& w2) {
+    constexpr uint32_t kWps = 32u / sizeof(Word);  // words per 32-byte sector
+    constexpr uint32_t kLwps = sizeof(Word) == 8 ? 2u : 3u;
+    if (vec32 && bb >= kLwps) {
+      const uint32_t s1 = i1 >> kLwps;
+      unsigned long long v[4];
+      ld_nc_256(p + (s1 << kLwps), v[0], v[1], v[2], v[3]);
+      w1 = pick(v, i1 & (kWps - 1u));
+      w2 = (i2 >> kLwps) == s1 ? pick(v, i2 & (kWps - 1u)) : __ldg(p + i2);
+    } else if (bb == 0) {
+      w1 = w2 = __ldg(p);
+    } else {
+      w1 = __ldg(p + i1);
+      w2 = __ldg(p + i2);
+    }
+  }
+
   __device__ __forceinline__ static bool contains(const ProbeArgs& a, uint32_t key) {
     uint32_t hv;
     const uint32_t blk = block_hash(key, a.addr, a.bcf_hash_shift, hv);
@@ -124,8 +158,8 @@ struct BcfOps {
     uint32_t i1, i2, tag;
     bucket_tag(hv, a.bcf_bucket_bits, i1, i2, tag);
     const Word* p = static_cast<const Word*>(a.filter) + (static_cast<uint64_t>(blk) << a.bcf_bucket_bits);
-    const Word w1 = __ldg(p + i1);
-    const Word w2 = __ldg(p + i2);
+    Word w1, w2;
+    load_pair(p, i1, i2, a.bcf_bucket_bits, a.vec32 != 0u, w1, w2);
     return (w1 == static_cast<Word>(Cfg::kOverflow)) | (w2 == static_cast<Word>(Cfg::kOverflow)) | has(w1, tag) |
            has(w2, tag);
   }

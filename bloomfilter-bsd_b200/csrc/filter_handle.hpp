@@ -10,6 +10,7 @@ struct dtlg_filter {
   const dtlg::BloomKernels* bk = nullptr;
   const dtlg::CuckooKernels* ck = nullptr;
   const dtlg::BcfKernels* xk = nullptr;   // blocked cuckoo
+  const dtlg::ClassicKernels* qk = nullptr;  // classic Bloom
   const dtlg::ProbeKernels* pk = nullptr;  // the probe kernels of whichever kind
   // probe tuning (dtlg_set_probe_options): mode 0 = auto, 1 = fused single
   // kernel, 2 = bitmask + compaction; bits_variant -1 = auto
@@ -25,5 +26,8 @@ inline void set_filter_args(const FilterDesc& d, ProbeArgs* a) {
   a->victim_word = d.victim_word;
   a->bcf_bucket_bits = d.bucket_bits;
   a->bcf_hash_shift = d.hash_shift;
+  a->cbf_k = d.k;
+  a->cbf_bit_shift = d.bit_shift;
+  a->cbf_bit_mask = d.bit_mask;
 }
 }  // namespace dtlg

@@ -156,9 +156,42 @@ int describe_bcf(uint32_t block_bytes, uint32_t t, uint32_t a, uint64_t m, Filte
   return 0;
 }
 
+int describe_classic(uint32_t k, uint64_t m, bool magic, FilterDesc* d) {
+  *d = FilterDesc{};
+  // dyn::mul32 throws for hash numbers above 16 (hash_family.hpp:295-297),
+  // from inside the reference's noexcept insert / contains: k <= 17
+  if (k > 17) return 1;
+  d->kind = Kind::kClassicBloom;
+  d->k = k;
+  d->m = m;
+  d->word_bytes = 4;
+  d->w = 1;
+  const int rc = make_addr((m + 31) / 32, magic, &d->addr);  // bloomfilter_logic.hpp:62-64
+  if (rc) return rc;
+  d->word_cnt = d->addr.block_cnt;                  // :84-87
+  d->m_actual = static_cast<uint64_t>(d->addr.block_cnt) * 32;  // :74-77
+  // bit index (h >> (27 - addressing bits)) & 31 (:105,138), as the reference
+  // compiles: a POW2 shift count taken mod 32, the MAGIC bit index 0
+  if (magic) {
+    d->bit_shift = 0;
+    d->bit_mask = 0;
+  } else {
+    d->bit_shift = (27u - ilog2(d->addr.block_cnt)) & 31u;
+    d->bit_mask = 31;
+  }
+  d->size_u64 = (d->word_cnt + 1) / 2;
+  d->alloc_u64 = d->size_u64;
+  return 0;
+}
+
 std::string filter_name(const FilterDesc& d) {
   const std::string addr = d.addr.magic_mode ? "\"magic\"" : "\"pow2\"";
   const uint64_t bytes = (d.m_actual + 7) / 8;
+  if (d.kind == Kind::kClassicBloom) {
+    // the reference's bloomfilter_logic has no name(): the blocked filters' format
+    return "{\"name\":\"bloom\",\"size\":" + std::to_string(bytes) + ",\"k\":" + std::to_string(d.k) +
+           ",\"addr\":" + addr + "}";
+  }
   if (d.kind == Kind::kBlockedCuckoo) {
     // blocked_cuckoofilter.hpp:445-454
     return "{\"name\":\"blocked_cuckoo\", \"size\":" + std::to_string(bytes) +

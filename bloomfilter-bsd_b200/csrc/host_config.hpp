@@ -1,7 +1,7 @@
 // host_config.hpp -- filter construction rules on the host (validation, sizes,
 // addressing, name).  Reference: blocked_bloomfilter.hpp:96-390,
 // zoned_blocked_bloomfilter.hpp:98-378, cuckoofilter.hpp:115-343,
-// blocked_cuckoofilter.hpp:183-455,
+// blocked_cuckoofilter.hpp:183-455, bloomfilter_logic.hpp:59-87,
 // block_addressing_logic.hpp:41-235, div.hpp:30-57, filter.hpp:42-72.
 #pragma once
 
@@ -12,7 +12,7 @@
 
 namespace dtlg {
 
-enum class Kind : int { kBloom = 0, kZoned = 1, kCuckoo = 2, kBlockedCuckoo = 3 };
+enum class Kind : int { kBloom = 0, kZoned = 1, kCuckoo = 2, kBlockedCuckoo = 3, kClassicBloom = 4 };
 
 // Smallest d >= max(n, 2) whose libdivide u32 magic needs neither the add step
 // nor the power-of-two shift path (div.hpp:30-57; libdivide.h:719-769, the
@@ -33,6 +33,8 @@ struct FilterDesc {
   // (32: the bucket hash is key * C[0]); word_bytes / w hold the bucket word
   // size and the buckets per block
   uint32_t block_bytes = 0, bucket_bits = 0, hash_shift = 32;
+  // classic Bloom: bit index = (h >> bit_shift) & bit_mask (k above)
+  uint32_t bit_shift = 0, bit_mask = 0;
   uint64_t m = 0, m_actual = 0;
   Addr addr{};
   uint64_t word_cnt = 0;      // Bloom: words of word_bytes; cuckoo: 32-bit table words
@@ -46,6 +48,7 @@ int describe_bloom(uint32_t word_size, uint32_t w, uint32_t s, uint32_t z, uint3
                    FilterDesc* out);
 int describe_cuckoo(uint32_t t, uint32_t b, uint64_t m, FilterDesc* out);
 int describe_bcf(uint32_t block_bytes, uint32_t t, uint32_t a, uint64_t m, FilterDesc* out);
+int describe_classic(uint32_t k, uint64_t m, bool magic, FilterDesc* out);
 std::string filter_name(const FilterDesc& d);
 
 }  // namespace dtlg

@@ -43,6 +43,8 @@ struct ProbeArgs {
   // blocked cuckoo filter: log2(buckets per block), and the shift that turns
   // the block hash into the bucket hash (32: the bucket hash is key * C[0])
   uint32_t bcf_bucket_bits, bcf_hash_shift;
+  // classic Bloom filter: bits per key, and the bit index (h >> shift) & mask
+  uint32_t cbf_k, cbf_bit_shift, cbf_bit_mask;
 };
 
 constexpr int kProbeThreads = 256;

@@ -7,6 +7,7 @@
 
 #include "bcf.cuh"
 #include "bloom.cuh"
+#include "classic.cuh"
 #include "cuckoo.cuh"
 #include "probe.cuh"
 #include "probe2.cuh"
@@ -57,10 +58,17 @@ struct BcfKernels {
   cudaError_t (*insert)(const BcfBuildArgs&, int grid, cudaStream_t);
 };
 
+struct ClassicKernels {
+  ProbeKernels pk;
+  cudaError_t (*build)(const ClassicBuildArgs&, int grid, cudaStream_t);
+};
+
 void register_bloom(const BloomKernels& k);
 void register_cuckoo(const CuckooKernels& k);
 void register_bcf(const BcfKernels& k);
 const BcfKernels* find_bcf(uint32_t t, uint32_t a);
+void register_classic(const ClassicKernels& k);
+const ClassicKernels* find_classic();
 const BloomKernels* find_bloom(uint32_t word_bytes, uint32_t w, uint32_t s, uint32_t z, uint32_t k);
 const CuckooKernels* find_cuckoo(uint32_t t, uint32_t b);
 int registered_bloom_count();

@@ -49,6 +49,10 @@ class BcfConfigS(C.Structure):
     _fields_ = [("block_size_bytes", C.c_uint32), ("tag_size_bits", C.c_uint32), ("associativity", C.c_uint32)]
 
 
+class ClassicConfigS(C.Structure):
+    _fields_ = [("k", C.c_uint32), ("addr_mode", C.c_uint32)]
+
+
 class BatchItemS(C.Structure):
     _fields_ = [("filter", C.c_void_p), ("filter_words", C.c_void_p), ("build_keys", C.c_void_p),
                 ("n_build", C.c_uint32), ("probe_keys", C.c_void_p), ("n_probe", C.c_uint32),
@@ -82,6 +86,7 @@ SIGNATURES = {
     "dtlg_bloom_create": (_i, [C.POINTER(BloomConfigS), _u64, C.POINTER(_vp)]),
     "dtlg_cuckoo_create": (_i, [C.POINTER(CuckooConfigS), _u64, C.POINTER(_vp)]),
     "dtlg_blocked_cuckoo_create": (_i, [C.POINTER(BcfConfigS), _u64, C.POINTER(_vp)]),
+    "dtlg_classic_bloom_create": (_i, [C.POINTER(ClassicConfigS), _u64, C.POINTER(_vp)]),
     "dtlg_destroy": (None, [_vp]),
     "dtlg_size_in_bytes": (_u64, [_vp]),
     "dtlg_size": (_u64, [_vp]),

@@ -113,7 +113,7 @@ class filter_base:  # noqa: N801 (reference name)
         return bool(lib().dtlg_is_magic(self._h))
 
     def kind(self):
-        return ("bloom", "zoned", "cuckoo", "blocked_cuckoo")[lib().dtlg_kind(self._h)]
+        return ("bloom", "zoned", "cuckoo", "blocked_cuckoo", "classic_bloom")[lib().dtlg_kind(self._h)]
 
     def set_probe_options(self, mode=0, variant=-1):
         """Probe kernel choice (0 auto, 1 fused, 2 bitmask + compaction) and the
@@ -308,6 +308,20 @@ class bcf(filter_base):  # noqa: N801 -- bcf.hpp:56, bcf.cpp:24-25
         super().__init__(h)
         self.block_size_bytes = block_size_bytes
         self.tag_size_bits, self.associativity = tag_size_bits, associativity
+
+
+class bloomfilter_logic(filter_base):  # noqa: N801 -- bloomfilter/bloomfilter_logic.hpp:22-64
+    """The classic Bloom filter: one bit in each of k independently addressed
+    32-bit words, k <= 17.  The addressing is the reference's template
+    argument (POWER_OF_TWO or MAGIC), not derived from m."""
+
+    def __init__(self, m, k, addressing=None):
+        addressing = POWER_OF_TWO if addressing is None else addressing
+        cfg = _lib.ClassicConfigS(k, 1 if addressing == MAGIC else 0)
+        h = C.c_void_p()
+        check(lib().dtlg_classic_bloom_create(C.byref(cfg), int(m), C.byref(h)), f"classic Bloom filter k={k}")
+        super().__init__(h)
+        self.k = k
 
 
 def construct(config, m):

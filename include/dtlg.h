@@ -78,6 +78,15 @@ typedef struct dtlg_blocked_cuckoo_config {
   uint32_t associativity;
 } dtlg_blocked_cuckoo_config;
 
+/* Mirrors dtl::bloomfilter_logic<uint32_t, addr_mode>(m, k), the classic
+ * Bloom filter (src/dtl/filter/bloomfilter/bloomfilter_logic.hpp:22-64): one
+ * bit in each of k 32-bit words.  The addressing is the template argument
+ * there (no dispatcher), so it is explicit here: 0 = POW2, 1 = MAGIC. */
+typedef struct dtlg_classic_bloom_config {
+  uint32_t k;         /* 0..17 (hash functions C[0..k-1], hash_family.hpp:271-299) */
+  uint32_t addr_mode;
+} dtlg_classic_bloom_config;
+
 typedef struct dtlg_filter dtlg_filter;
 
 /* ---- construction (filter.hpp:42-72; bbf_32.hpp:53, zbbf_*.hpp, cf.hpp) ---- */
@@ -89,6 +98,10 @@ dtlg_status dtlg_cuckoo_create(const dtlg_cuckoo_config* cfg, uint64_t m_bits, d
  * of that; blocks are >= 8 bytes) like every other kind. */
 dtlg_status dtlg_blocked_cuckoo_create(const dtlg_blocked_cuckoo_config* cfg, uint64_t m_bits,
                                        dtlg_filter** out);
+/* dtl::bloomfilter_logic<uint32_t, A>::bloomfilter_logic(m, k)
+ * (bloomfilter_logic.hpp:62-64).  k > 17 is rejected here; the reference
+ * throws from inside its noexcept insert / contains (std::terminate). */
+dtlg_status dtlg_classic_bloom_create(const dtlg_classic_bloom_config* cfg, uint64_t m_bits, dtlg_filter** out);
 void dtlg_destroy(dtlg_filter* f);
 
 /* ---- sizes and name ---- */
@@ -105,14 +118,16 @@ uint64_t dtlg_alloc_words_u64(const dtlg_filter* f);
  * cuckoofilter.hpp:335-343, blocked_cuckoofilter.hpp:445-454).  Writes a NUL-terminated string; returns its
  * length (excluding NUL) or the required length if cap is too small. */
 size_t dtlg_name(const dtlg_filter* f, char* buf, size_t cap);
-/* Introspection: 0 = Bloom, 1 = zoned Bloom, 2 = cuckoo, 3 = blocked cuckoo;
+/* Introspection: 0 = Bloom, 1 = zoned Bloom, 2 = cuckoo, 3 = blocked cuckoo,
+ * 4 = classic Bloom;
  * block (bucket) count; 1 if MAGIC addressing. */
 int dtlg_kind(const dtlg_filter* f);
 uint64_t dtlg_block_cnt(const dtlg_filter* f);
 int dtlg_is_magic(const dtlg_filter* f);
 
 /* ---- build: filter_base::batch_insert (filter_base.hpp:26) ---- */
-/* Bloom and blocked cuckoo: always DTLG_OK on valid input (bbf_32.cpp:41-45,
+/* Bloom, classic Bloom and blocked cuckoo: always DTLG_OK on valid input
+ * (bbf_32.cpp:41-45, bloomfilter_logic.hpp:115-121,
  * bcf.cpp:36-40; a blocked cuckoo key that finds no slot marks its bucket
  * overflowed, block_logic.hpp:117).  Cuckoo: returns
  * DTLG_ERR_CUCKOO_FULL when some key could not be placed (the reference's

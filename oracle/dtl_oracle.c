@@ -664,3 +664,65 @@ uint64_t orc_bcf_batch_contains(const orc_bcf *f, const void *data, const uint32
     if (orc_bcf_contains(f, data, keys[i])) match_pos[cnt++] = i + match_offset;
   return cnt;
 }
+
+/* ======================================================================== */
+/* Classic Bloom filter                                                      */
+/* ======================================================================== */
+
+/* bloomfilter_logic.hpp:62-64: one addressing "block" per 32-bit word.  The
+ * bit index is (h >> (32 - 5 - addressing bits)) & 31 (:105,138), a shift the
+ * C++ leaves undefined once the addressing bits exceed 27.  Restated as the
+ * reference compiles (g++ 13, x86-64, -O2; pinned by tests against
+ * oracle/_ref): with POW2 the shift count is a run-time value and x86 takes it
+ * mod 32; with MAGIC the addressing bits are the constant 32 and the compiler
+ * folds the bit index to 0. */
+int orc_cbf_init(orc_cbf *f, uint32_t k, uint64_t m, uint32_t mode) {
+  memset(f, 0, sizeof(*f));
+  if (k > 17) return ORC_ERR_CONFIG;   /* dyn::mul32 throws for hash_no > 16 (hash_family.hpp:295-297) */
+  f->k = k;
+  f->m = m;
+  int rc = orc_addr_init(&f->addr, (m + 31) / 32, mode);
+  if (rc) return rc;
+  f->word_cnt = f->addr.block_cnt;                      /* :84-87 */
+  f->m_actual = (uint64_t)f->addr.block_cnt * 32;       /* :74-77 */
+  if (mode == ORC_ADDR_MAGIC) {
+    f->bit_shift = 0;
+    f->bit_mask = 0;
+  } else {
+    f->bit_shift = (27u - f->addr.block_cnt_log2) & 31u;
+    f->bit_mask = 31;
+  }
+  return ORC_OK;
+}
+
+static uint32_t cbf_bit(const orc_cbf *f, uint32_t h) { return (h >> f->bit_shift) & f->bit_mask; }
+
+/* :94-121 */
+void orc_cbf_insert(const orc_cbf *f, void *data, const uint32_t *keys, uint64_t n) {
+  uint32_t *w = (uint32_t *)data;
+  for (uint64_t x = 0; x < n; x++) {
+    for (uint32_t i = 0; i < f->k; i++) {
+      const uint32_t h = keys[x] * kMul[i];            /* dyn::mul32 (hash_family.hpp:271-299) */
+      w[orc_addr_block(&f->addr, h)] |= 1u << cbf_bit(f, h);
+    }
+  }
+}
+
+/* :127-144, with its early out */
+int orc_cbf_contains(const orc_cbf *f, const void *data, uint32_t key) {
+  const uint32_t *w = (const uint32_t *)data;
+  for (uint32_t i = 0; i < f->k; i++) {
+    const uint32_t h = key * kMul[i];
+    if (!((w[orc_addr_block(&f->addr, h)] >> cbf_bit(f, h)) & 1u)) return 0;
+  }
+  return 1;
+}
+
+/* :188-208 */
+uint64_t orc_cbf_batch_contains(const orc_cbf *f, const void *data, const uint32_t *keys,
+                                uint32_t n, uint32_t *match_pos, uint32_t match_offset) {
+  uint64_t cnt = 0;
+  for (uint32_t i = 0; i < n; i++)
+    if (orc_cbf_contains(f, data, keys[i])) match_pos[cnt++] = i + match_offset;
+  return cnt;
+}

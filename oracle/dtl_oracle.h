@@ -139,6 +139,26 @@ uint64_t orc_bcf_batch_contains(const orc_bcf *f, const void *data, const uint32
 void orc_bcf_locate(const orc_bcf *f, uint32_t key, uint32_t *block, uint32_t *b1, uint32_t *b2,
                     uint32_t *tag);
 
+/* ---------------------------------------------------------------------------
+ * Classic Bloom filter (bloomfilter/bloomfilter_logic.hpp:22-212): one bit in
+ * each of k independently addressed 32-bit words.
+ * ------------------------------------------------------------------------- */
+typedef struct {
+  uint32_t k;               /* bits per key, 0..17 (hash functions C[0..k-1]) */
+  orc_addr addr;            /* one "block" per 32-bit word */
+  uint32_t bit_shift;       /* bit index = (h >> bit_shift) & bit_mask */
+  uint32_t bit_mask;
+  uint64_t m, m_actual;
+  uint64_t word_cnt;        /* bloomfilter_logic::size(): 32-bit words */
+} orc_cbf;
+
+/* mode: ORC_ADDR_POW2 or ORC_ADDR_MAGIC (the reference's template argument). */
+int orc_cbf_init(orc_cbf *f, uint32_t k, uint64_t m, uint32_t mode);
+void orc_cbf_insert(const orc_cbf *f, void *data, const uint32_t *keys, uint64_t n);
+int orc_cbf_contains(const orc_cbf *f, const void *data, uint32_t key);
+uint64_t orc_cbf_batch_contains(const orc_cbf *f, const void *data, const uint32_t *keys,
+                                uint32_t n, uint32_t *match_pos, uint32_t match_offset);
+
 /* Parallel (pthreads) batch_contains over contiguous slices; used only as the
  * timed CPU baseline.  Returns the total match count; per-slice positions are
  * written to match_pos[slice_begin ...] (not compacted). */

@@ -3,11 +3,12 @@
 TEST INFRASTRUCTURE ONLY: imported by tests/, by __graft_entry__.smoke() and by
 bench.py's CPU-baseline / reference legs, never by the product package.
 
-* ``Bloom`` / ``Cuckoo`` / ``BlockedCuckoo`` wrap liboracle.so, the C
-  restatement (dtl_oracle.c).
+* ``Bloom`` / ``Cuckoo`` / ``BlockedCuckoo`` / ``ClassicBloom`` wrap
+  liboracle.so, the C restatement (dtl_oracle.c).
 * ``RefLib`` wraps oracle/_ref/libdtlref_*.so, the reference's own filter logic
   compiled from its sources (see oracle/Makefile); absent when not built.
-  ``RefBcf`` wraps oracle/_ref/libdtlref_bcf*.so, the reference's dtl::bcf.
+  ``RefBcf`` wraps oracle/_ref/libdtlref_bcf*.so, the reference's dtl::bcf;
+  ``RefCbf`` oracle/_ref/libdtlref_cbf.so, its classic Bloom filter.
 """
 import ctypes as C
 import os
@@ -39,6 +40,11 @@ class _BcfS(C.Structure):
     _fields_ = [("block_bytes", C.c_uint32), ("t", C.c_uint32), ("a", C.c_uint32), ("word_bytes", C.c_uint32),
                 ("bucket_bits", C.c_uint32), ("hash_shift", C.c_uint32), ("addr", _Addr), ("m", C.c_uint64),
                 ("m_actual", C.c_uint64), ("word_cnt", C.c_uint64), ("size_u32", C.c_uint64)]
+
+
+class _CbfS(C.Structure):
+    _fields_ = [("k", C.c_uint32), ("addr", _Addr), ("bit_shift", C.c_uint32), ("bit_mask", C.c_uint32),
+                ("m", C.c_uint64), ("m_actual", C.c_uint64), ("word_cnt", C.c_uint64)]
 
 
 _lib = None
@@ -91,6 +97,13 @@ def lib():
         L.orc_bcf_batch_contains.restype = C.c_uint64
         L.orc_bcf_batch_contains.argtypes = [C.POINTER(_BcfS), C.c_void_p, _u32p, C.c_uint32, _u32p, C.c_uint32]
         L.orc_bcf_locate.argtypes = [C.POINTER(_BcfS), C.c_uint32] + [C.POINTER(C.c_uint32)] * 4
+        L.orc_cbf_init.restype = C.c_int
+        L.orc_cbf_init.argtypes = [C.POINTER(_CbfS), C.c_uint32, C.c_uint64, C.c_uint32]
+        L.orc_cbf_insert.argtypes = [C.POINTER(_CbfS), C.c_void_p, _u32p, C.c_uint64]
+        L.orc_cbf_contains.restype = C.c_int
+        L.orc_cbf_contains.argtypes = [C.POINTER(_CbfS), C.c_void_p, C.c_uint32]
+        L.orc_cbf_batch_contains.restype = C.c_uint64
+        L.orc_cbf_batch_contains.argtypes = [C.POINTER(_CbfS), C.c_void_p, _u32p, C.c_uint32, _u32p, C.c_uint32]
         _lib = L
     return _lib
 
@@ -274,6 +287,45 @@ class BlockedCuckoo:
         r = [C.c_uint32() for _ in range(4)]
         lib().orc_bcf_locate(C.byref(self.s_), int(key), *[C.byref(x) for x in r])
         return tuple(x.value for x in r)  # block, bucket 1, bucket 2, tag
+
+
+class ClassicBloom:
+    """C restatement of the classic Bloom filter (data owned by caller)."""
+
+    def __init__(self, k, m, magic=False):
+        self.s_ = _CbfS()
+        rc = lib().orc_cbf_init(C.byref(self.s_), k, m, 1 if magic else 0)
+        if rc:
+            raise ValueError(f"invalid classic Bloom config rc={rc}")
+
+    @property
+    def word_cnt(self):
+        return self.s_.word_cnt
+
+    @property
+    def m_actual(self):
+        return self.s_.m_actual
+
+    @property
+    def block_cnt(self):
+        return self.s_.addr.block_cnt
+
+    def alloc(self):
+        return np.zeros(max(1, (self.word_cnt + 1) // 2), dtype=np.uint64)
+
+    def insert(self, data, keys):
+        k = _keys(keys)
+        lib().orc_cbf_insert(C.byref(self.s_), data.ctypes.data, k, len(k))
+
+    def contains(self, data, key):
+        return bool(lib().orc_cbf_contains(C.byref(self.s_), data.ctypes.data, int(key)))
+
+    def batch_contains(self, data, keys, match_offset=0):
+        k = _keys(keys)
+        out = np.zeros(max(1, len(k)), dtype=np.uint32)
+        n = lib().orc_cbf_batch_contains(C.byref(self.s_), data.ctypes.data, k, len(k), out,
+                                         match_offset & 0xFFFFFFFF)
+        return out[:n].copy()
 
 
 # --------------------------------------------------------------------------
@@ -487,5 +539,80 @@ class _RefBcfFilter:
 def try_refbcf(variant="scalar"):
     try:
         return RefBcf(variant)
+    except (FileNotFoundError, OSError):
+        return None
+
+
+class RefCbf:
+    """The reference's classic Bloom filter (oracle/_ref/libdtlref_cbf.so)."""
+
+    def __init__(self):
+        path = os.path.join(HERE, "_ref", "libdtlref_cbf.so")
+        if not os.path.exists(path):
+            raise FileNotFoundError(path)
+        self.path = path
+        L = C.CDLL(path)
+        vp = C.c_void_p
+        L.ref_cbf_create.restype = vp
+        L.ref_cbf_create.argtypes = [C.c_uint64, C.c_uint32, C.c_uint32]
+        L.ref_cbf_destroy.argtypes = [vp]
+        L.ref_cbf_size.restype = C.c_uint64
+        L.ref_cbf_size.argtypes = [vp]
+        L.ref_cbf_length.restype = C.c_uint64
+        L.ref_cbf_length.argtypes = [vp]
+        L.ref_cbf_batch_insert.restype = C.c_int
+        L.ref_cbf_batch_insert.argtypes = [vp, vp, _u32p, C.c_uint32]
+        L.ref_cbf_batch_contains.restype = C.c_uint64
+        L.ref_cbf_batch_contains.argtypes = [vp, vp, _u32p, C.c_uint32, _u32p, C.c_uint32]
+        L.ref_cbf_batch_contains_mt.restype = C.c_uint64
+        L.ref_cbf_batch_contains_mt.argtypes = [vp, vp, _u32p, C.c_uint64, _u32p, C.c_int]
+        self.L = L
+
+    def create(self, k, m, magic=False):
+        h = self.L.ref_cbf_create(m, k, 1 if magic else 0)
+        return _RefCbfFilter(self, h) if h else None
+
+
+class _RefCbfFilter:
+    def __init__(self, ref, h):
+        self.ref, self.h = ref, h
+
+    def __del__(self):
+        try:
+            self.ref.L.ref_cbf_destroy(self.h)
+        except Exception:
+            pass
+
+    @property
+    def size_u32(self):
+        return self.ref.L.ref_cbf_size(self.h)
+
+    @property
+    def length(self):
+        return self.ref.L.ref_cbf_length(self.h)
+
+    def alloc(self):
+        return np.zeros(self.size_u32 + 16, dtype=np.uint32)
+
+    def insert(self, data, keys):
+        k = _keys(keys)
+        return bool(self.ref.L.ref_cbf_batch_insert(self.h, data.ctypes.data, k, len(k)))
+
+    def batch_contains(self, data, keys, match_offset=0):
+        k = _keys(keys)
+        out = np.zeros(len(k) + 16, dtype=np.uint32)
+        n = self.ref.L.ref_cbf_batch_contains(self.h, data.ctypes.data, k, len(k), out, match_offset & 0xFFFFFFFF)
+        return out[:n].copy()
+
+    def batch_contains_mt(self, data, keys, threads, out=None):
+        k = _keys(keys)
+        if out is None:
+            out = np.zeros(len(k) + 16, dtype=np.uint32)
+        return self.ref.L.ref_cbf_batch_contains_mt(self.h, data.ctypes.data, k, len(k), out, threads)
+
+
+def try_refcbf():
+    try:
+        return RefCbf()
     except (FileNotFoundError, OSError):
         return None

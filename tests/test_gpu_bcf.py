@@ -75,6 +75,26 @@ def test_probe_reference_fixtures(bcf_golden):
             assert np.array_equal(got, exp), (e["id"], mode)
 
 
+def test_probe_filter_not_32_byte_aligned(bcf_golden):
+    """A filter base that is 16- but not 32-byte aligned takes the word-load
+    path instead of the 256-bit sector loads; results are the same."""
+    index, arr = bcf_golden
+    for e in index["bcf"][::3]:
+        f = F.bcf(e["m"], e["block_bytes"], e["t"], e["a"])
+        n64 = f.alloc_words()
+        buf = torch.zeros(n64 + 4, dtype=torch.int64, device="cuda")
+        w = buf[2:2 + n64]
+        assert w.data_ptr() % 32 == 16
+        t = np.zeros(n64 * 2, dtype=np.uint32)
+        t[: len(arr[f"bcf_{e['id']}_table"])] = arr[f"bcf_{e['id']}_table"]
+        w.copy_(torch.from_numpy(t.view(np.int64)))
+        pk, _ = keygen.probe_keys(e["n_build"], e["n_probe"], e["hit_ratio"], e["seed"])
+        for mode in (1, 2, 3):
+            f.set_probe_options(mode, -1)
+            got = gpu_probe(f, w, pk, e["match_offset"])
+            assert np.array_equal(got, arr[f"bcf_{e['id']}_hits"]), (e["id"], mode)
+
+
 def test_build_invariants_every_config():
     for ci, (bb, (t, a)) in enumerate([(bb, ta) for bb in BLOCKS for ta in TAG_PAIRS]):
         for m in (1 << 17, 100003):
