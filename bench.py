@@ -37,6 +37,9 @@ WORKLOADS = {
     # 2^26 probes: the case ncu captures run on
     "sectorized_dram_small": (8, 8, 8, 1, 8, 27, 16, 26, 0.10),
     "register_blocked": (4, 1, 1, 1, 4, 20, 16, 24, 0.10),
+    # a 64 KiB filter (2^15 keys): L1-resident; --probe-mode 4 probes a copy
+    # in every CTA's shared memory instead
+    "sectorized_small": (8, 8, 8, 1, 8, 15, 16, 28, 0.10),
 }
 CUCKOO_WORKLOADS = {
     # name: (bits per tag, tags per bucket, log2 n, load factor, log2 probes, hit ratio)
@@ -65,7 +68,7 @@ def parse():
     ap.add_argument("--batch-max-log2", type=int, default=24, help="batched512: log2 of the largest n / probes")
     ap.add_argument("--no-e2e", action="store_true")
     ap.add_argument("--probe-mode", type=int, default=0,
-                    help="0 auto, 1 fused, 2 bitmask + block-range passes, 3 partitioned")
+                    help="0 auto, 1 fused, 2 bitmask + block-range passes, 3 partitioned, 4 shared-memory filter copy")
     ap.add_argument("--probe-passes", type=int, default=0, help="block-range passes of mode 2 (0 auto)")
     return ap.parse_args()
 

@@ -188,21 +188,31 @@ dtlg_status check_filter_ptr(const void* p) {
 // Probe kernel plan for n keys: 1 = fused (probe + ordered compaction in one
 // kernel), 2 = match bitmask in block-range passes + compaction,
 // 3 = partitioned probe (Bloom and blocked cuckoo filters: one block per key)
-// + compaction.
+// + compaction, 4 = match bitmask against a shared-memory copy of a filter of
+// at most kSmemMaxBytes (Bloom and classic Bloom filters) + compaction.
 // Automatic choice (measured on B200, u64 w=8 s=8 k=8, 2^26-2^28 probes):
 // below 2^20 keys the single fused kernel; Bloom filters above 160 MiB the
 // partitioned probe (256 MiB: 68.6 vs 62.5 Gkeys/s; 512 MiB: 64 vs 54); else
 // the bitmask kernel (L2-resident filters: 113 vs 76 Gkeys/s partitioned).
+// Plan 4 is offered up to kSmemMaxBytes (below every sm_100 opt-in limit,
+// 227 KiB) but never chosen automatically: on B200 a small filter read through
+// L1 probes faster than a shared-memory copy (64 KiB u64 w=8 s=8 k=8 filter,
+// 2^28 probes: 141.5 Gkeys/s plan 2, 101.5 plan 4 -- random 16-byte shared
+// loads conflict on banks, L1 hits do not).  The autotuner times it.
+constexpr uint64_t kSmemMaxBytes = 192ull << 10;
+
 int probe_plan(const dtlg_filter* f, uint64_t n) {
   int mode = f->probe_mode;
   const bool partitioned = f->pk->probe_pairs[0] != nullptr;
+  const uint64_t fbytes = (f->d.m_actual + 7) / 8;
+  const bool smem = f->pk->probe_smem != nullptr && fbytes <= kSmemMaxBytes;
   if (mode == 3 && !partitioned) mode = 2;
+  if (mode == 4 && !smem) mode = 2;
   if (mode == 0) {
-    const uint64_t bytes = (f->d.m_actual + 7) / 8;
     if (n < kTwoPassMinKeys) {
       mode = 1;
     } else {
-      mode = (partitioned && bytes > (160ull << 20)) ? 3 : 2;
+      mode = (partitioned && fbytes > (160ull << 20)) ? 3 : 2;
     }
   }
   return mode;
@@ -276,7 +286,11 @@ dtlg_status launch_probe(const dtlg_filter* f, const uint64_t* words, const uint
   uint32_t* bits = reinterpret_cast<uint32_t*>(wsb + lay.bits_off);
   const int v = (f->bits_variant >= 0 && f->bits_variant < kBitsVariants) ? f->bits_variant : 1;
   a.vec32 = (reinterpret_cast<uintptr_t>(words) & 31u) == 0 ? 1u : 0u;
-  if (mode == 2) {
+  if (mode == 4) {
+    // the whole filter in every CTA's shared memory
+    const uint32_t words32 = static_cast<uint32_t>((f->d.m_actual + 31) / 32);
+    DTLG_CUDA(f->pk->probe_smem(a, bits, words32, (n_phys + 127) / 128, ds->sms, stream));
+  } else if (mode == 2) {
     // match bitmask, in block-range passes over large filters (each pass
     // probes only the keys whose block lies in its range, so the concurrently
     // touched part of the filter stays within the GPU's address-translation reach)
@@ -598,7 +612,7 @@ dtlg_status dtlg_set_l2_fetch_granularity(int bytes, int* in_effect) {
 int dtlg_probe_kernel_count(const dtlg_filter* f, uint32_t key_cnt) {
   if (!f || key_cnt == 0) return 0;
   const int mode = probe_plan(f, key_cnt);
-  return mode == 1 ? 1 : (mode == 2 ? static_cast<int>(probe_passes(f)) + 1 : 5);
+  return mode == 1 ? 1 : (mode == 2 ? static_cast<int>(probe_passes(f)) + 1 : (mode == 4 ? 2 : 5));
 }
 
 dtlg_status dtlg_set_probe_passes(dtlg_filter* f, int passes) {
@@ -610,7 +624,7 @@ dtlg_status dtlg_set_probe_passes(dtlg_filter* f, int passes) {
 
 dtlg_status dtlg_set_probe_options(dtlg_filter* f, int mode, int variant) {
   if (!f) return DTLG_ERR_NULL;
-  if (mode < 0 || mode > 3 || variant < -1 || variant >= kBitsVariants) return DTLG_ERR_INVALID_CONFIG;
+  if (mode < 0 || mode > 4 || variant < -1 || variant >= kBitsVariants) return DTLG_ERR_INVALID_CONFIG;
   f->probe_mode = mode;
   f->bits_variant = variant;
   return DTLG_OK;

@@ -6,8 +6,8 @@
 // (blocked_bloomfilter_tune_impl.hpp:162-268, cuckoofilter_tune_impl.hpp:
 // 118-225).  Here the alternatives are the probe plans -- the fused kernel,
 // the bitmask kernel in one or more block-range passes with either register
-// budget, and (Bloom and blocked cuckoo filters beyond 32 MiB) the
-// partitioned probe -- and the
+// budget, (Bloom and blocked cuckoo filters beyond 32 MiB) the partitioned
+// probe, and (Bloom filters of at most 192 KiB) the shared-memory probe -- and the
 // choice is stored on the filter handle.  Every plan must report the same
 // match count; a disagreement is returned as an error.
 #include <cuda_runtime.h>
@@ -34,6 +34,7 @@ std::vector<Plan> candidate_plans(const dtlg_filter* f, uint32_t n) {
     if (bytes > (512ull << 20)) passes.push_back(8);
     for (int v = 0; v < dtlg::kBitsVariants; v++)
       for (int p : passes) out.push_back({2, v, p});
+    if (f->pk->probe_smem && bytes <= (192ull << 10)) out.push_back({4, -1, 0});
     if (f->pk->probe_pairs[0] && bytes > (32ull << 20))
       for (int v = 0; v < dtlg::kBitsVariants; v++) out.push_back({3, v, 0});
   }

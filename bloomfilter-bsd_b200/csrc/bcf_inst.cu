@@ -29,8 +29,8 @@ cudaError_t classic_build(const ClassicBuildArgs& a, int grid, cudaStream_t s) {
 }
 
 // The classic Bloom filter's k words lie anywhere in the filter: no
-// partitioned plan.
-ClassicKernels classic_entry() { return ClassicKernels{probe_entry<ClassicOps, false>(), &classic_build}; }
+// partitioned plan; small filters take the shared-memory plan.
+ClassicKernels classic_entry() { return ClassicKernels{probe_entry<ClassicOps, false, true>(), &classic_build}; }
 
 struct RegBcf {
   RegBcf() {

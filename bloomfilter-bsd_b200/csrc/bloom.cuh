@@ -189,6 +189,41 @@ struct BloomOps {
     return ok;
   }
 
+  // The same test against a copy of the filter in shared memory (plan 4):
+  // plain loads, which the compiler issues as shared-memory loads.
+  __device__ __forceinline__ static bool contains_shared(const void* sfilter, const ProbeArgs& a, uint32_t key) {
+    const uint32_t blk = block_index(key * mul_const(0), a.addr);
+    const Word* base = static_cast<const Word*>(sfilter) + static_cast<uint64_t>(blk) * kW;
+    constexpr int kBytes = kW * static_cast<int>(sizeof(Word));
+    bool ok = true;
+    if constexpr (kS.fixed_words) {
+      Word v[kW];
+      if constexpr (kBytes >= 16) {
+#pragma unroll
+        for (int i = 0; i < kBytes / 16; i++) {
+          const uint4 x = reinterpret_cast<const uint4*>(base)[i];
+          uint32_t* d = reinterpret_cast<uint32_t*>(&v[0]) + 4 * i;
+          d[0] = x.x; d[1] = x.y; d[2] = x.z; d[3] = x.w;
+        }
+      } else {
+#pragma unroll
+        for (int i = 0; i < kW; i++) v[i] = base[i];
+      }
+      static_for<kS.ng>([&](auto G) {
+        constexpr int g = decltype(G)::value;
+        const Word m = group_mask<g>(key);
+        ok &= (v[kS.g[g].wconst] & m) == m;
+      });
+    } else {
+      static_for<kS.ng>([&](auto G) {
+        constexpr int g = decltype(G)::value;
+        const Word m = group_mask<g>(key);
+        ok &= (base[group_word<g>(key)] & m) == m;
+      });
+    }
+    return ok;
+  }
+
   __device__ __forceinline__ static void insert(void* filter, uint32_t key, const Addr& a) {
     Word* base = const_cast<Word*>(block_ptr(filter, key, a));
     static_for<kS.ng>([&](auto G) {

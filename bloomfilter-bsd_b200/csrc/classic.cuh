@@ -49,6 +49,20 @@ struct ClassicOps {
     }
     return hit;
   }
+
+  // The same test against a copy of the filter in shared memory (plan 4).
+  __device__ __forceinline__ static bool contains_shared(const void* sfilter, const ProbeArgs& a, uint32_t key) {
+    const unsigned int* w = static_cast<const unsigned int*>(sfilter);
+    bool hit = true;
+#pragma unroll
+    for (uint32_t i = 0; i < kClassicMaxK; i++) {
+      if (i >= a.cbf_k || !hit) break;
+      const uint32_t h = key * mul_const(static_cast<int>(i));
+      const uint32_t bit = (h >> a.cbf_bit_shift) & a.cbf_bit_mask;
+      hit = (w[block_index(h, a.addr)] >> bit) & 1u;
+    }
+    return hit;
+  }
 };
 
 #endif  // __CUDACC__

@@ -13,7 +13,8 @@ struct dtlg_filter {
   const dtlg::ClassicKernels* qk = nullptr;  // classic Bloom
   const dtlg::ProbeKernels* pk = nullptr;  // the probe kernels of whichever kind
   // probe tuning (dtlg_set_probe_options): mode 0 = auto, 1 = fused single
-  // kernel, 2 = bitmask + compaction; bits_variant -1 = auto
+  // kernel, 2 = bitmask + compaction, 3 = partitioned, 4 = shared-memory
+  // filter copy; bits_variant -1 = auto
   int probe_mode = 0;
   int bits_variant = -1;
   int probe_passes = 0;  // block-range passes of the two-pass probe; 0 = auto

@@ -3,7 +3,8 @@
 // 1. probe_bits_kernel: every warp takes chunks of 128 keys (one 16-byte key
 //    vector per lane), tests them, and writes the 128 match flags as four
 //    32-bit words of a key-ordered bitmask.  No barrier, no look-back: the only
-//    thing a warp ever waits for is its own filter loads.
+//    thing a warp ever waits for is its own filter loads.  probe_smem_kernel
+//    does the same against a copy of a small filter in shared memory.
 // 2. compact_kernel: turns the bitmask into the ascending position list.  A
 //    tile is 65536 keys (2048 mask words); the tile offset comes from a
 //    decoupled look-back (bounded waits, as in probe.cuh) over a few thousand
@@ -44,12 +45,14 @@ struct CompactArgs {
 
 #ifdef __CUDACC__
 
-// or_into: a later block-range pass ORs its flags into the words of the
-// earlier passes (every word is written by exactly one warp per pass, and the
-// passes are ordered on one stream).
-template <class Ops, int MINB>
-__global__ void __launch_bounds__(256, MINB)
-probe_bits_kernel(const __grid_constant__ ProbeArgs a, uint32_t* __restrict__ bits, int or_into) {
+// The bitmask loop: every warp takes chunks of 128 keys (one 16-byte key
+// vector per lane), tests them with test(key) and writes the 128 flags as four
+// 32-bit words of the key-ordered mask.  or_into: a later block-range pass ORs
+// its flags into the words of the earlier passes (every word is written by
+// exactly one warp per pass, and the passes are ordered on one stream).
+template <class Test>
+__device__ __forceinline__ void bits_loop(const ProbeArgs& a, uint32_t* __restrict__ bits, int or_into,
+                                          Test test) {
   const uint32_t lane = threadIdx.x & 31u;
   const uint4* keys4 = reinterpret_cast<const uint4*>(a.keys_al);
   const uint64_t n_vec = (a.n_phys + 3) >> 2;
@@ -64,7 +67,7 @@ probe_bits_kernel(const __grid_constant__ ProbeArgs a, uint32_t* __restrict__ bi
       const uint4 kv = __ldcs(keys4 + v);
       const uint32_t k[4] = {kv.x, kv.y, kv.z, kv.w};
 #pragma unroll
-      for (int q = 0; q < 4; q++) f |= (Ops::contains(a, k[q]) ? 1u : 0u) << q;
+      for (int q = 0; q < 4; q++) f |= (test(k[q]) ? 1u : 0u) << q;
       const uint64_t p0 = v * 4;
       if (p0 < a.pre || p0 + 4 > a.n_phys) {
 #pragma unroll
@@ -85,6 +88,32 @@ probe_bits_kernel(const __grid_constant__ ProbeArgs a, uint32_t* __restrict__ bi
       }
     }
   }
+}
+
+template <class Ops, int MINB>
+__global__ void __launch_bounds__(256, MINB)
+probe_bits_kernel(const __grid_constant__ ProbeArgs a, uint32_t* __restrict__ bits, int or_into) {
+  bits_loop(a, bits, or_into, [&](uint32_t key) { return Ops::contains(a, key); });
+}
+
+// Plan 4, filters that fit in shared memory: every CTA first copies the whole
+// filter (filter_words32 32-bit words) into shared memory with coalesced
+// loads, then runs the bitmask loop against that copy.  Random block reads
+// then cost shared-memory bank cycles instead of L1TEX tag lookups.
+constexpr int kSmemThreads = 512;
+
+template <class Ops>
+__global__ void __launch_bounds__(kSmemThreads)
+probe_smem_kernel(const __grid_constant__ ProbeArgs a, uint32_t* __restrict__ bits, uint32_t filter_words32) {
+  extern __shared__ uint4 s_filter[];
+  const uint32_t n_vec = filter_words32 >> 2;
+  const uint4* g4 = static_cast<const uint4*>(a.filter);
+  for (uint32_t i = threadIdx.x; i < n_vec; i += blockDim.x) s_filter[i] = __ldg(g4 + i);
+  uint32_t* s32 = reinterpret_cast<uint32_t*>(s_filter);
+  const uint32_t* g32 = static_cast<const uint32_t*>(a.filter);
+  for (uint32_t i = n_vec * 4 + threadIdx.x; i < filter_words32; i += blockDim.x) s32[i] = __ldg(g32 + i);
+  __syncthreads();
+  bits_loop(a, bits, 0, [&](uint32_t key) { return Ops::contains_shared(s_filter, a, key); });
 }
 
 static __global__ void __launch_bounds__(kCompactThreads) compact_kernel(const __grid_constant__ CompactArgs a) {

@@ -3,6 +3,7 @@
 
 #include <cuda_runtime.h>
 
+#include <algorithm>
 #include <cstdint>
 
 #include "bcf.cuh"
@@ -24,6 +25,10 @@ using probe_bits_fn = cudaError_t (*)(const ProbeArgs&, uint32_t* bits, int or_i
 // 1 = 4 CTAs/SM (64 registers, more filter loads in flight per thread).
 constexpr int kBitsVariants = 2;
 using pairs_fn = cudaError_t (*)(const PairsArgs&, int grid, cudaStream_t);
+// plan 4: bitmask probe against a shared-memory copy of a filter of words32
+// 32-bit words; chunks = 128-key chunks of the batch, sms = SM count
+using smem_fn = cudaError_t (*)(const ProbeArgs&, uint32_t* bits, uint32_t words32, uint64_t chunks, int sms,
+                                cudaStream_t);
 
 // The probe kernels every filter kind provides to the probe plans.
 struct ProbeKernels {
@@ -33,6 +38,7 @@ struct ProbeKernels {
   occ_fn bits_blocks_per_sm[kBitsVariants];
   pairs_fn probe_pairs[kBitsVariants];          // plan 3: partitioned (null: not offered)
   occ_fn pairs_blocks_per_sm[kBitsVariants];
+  smem_fn probe_smem;                           // plan 4: filter in shared memory (null: not offered)
 };
 
 struct BloomKernels {
@@ -125,8 +131,35 @@ struct BloomLaunch {
   }
 };
 
-// Probe kernels of one Ops type; Pairs = false leaves the partitioned plan out.
-template <class Ops, bool Pairs>
+template <class Ops>
+struct SmemLaunch {
+  static cudaError_t run(const ProbeArgs& a, uint32_t* bits, uint32_t words32, uint64_t chunks, int sms,
+                         cudaStream_t s) {
+    static const cudaError_t attr = [] {
+      int dev = 0, optin = 0;
+      cudaError_t e = cudaGetDevice(&dev);
+      if (e == cudaSuccess) e = cudaDeviceGetAttribute(&optin, cudaDevAttrMaxSharedMemoryPerBlockOptin, dev);
+      if (e == cudaSuccess)
+        e = cudaFuncSetAttribute(probe_smem_kernel<Ops>, cudaFuncAttributeMaxDynamicSharedMemorySize, optin);
+      return e;
+    }();
+    if (attr != cudaSuccess) return attr;
+    const size_t bytes = (static_cast<size_t>(words32) * 4 + 15) & ~static_cast<size_t>(15);
+    int occ = 0;
+    cudaError_t e = cudaOccupancyMaxActiveBlocksPerMultiprocessor(&occ, probe_smem_kernel<Ops>, kSmemThreads, bytes);
+    if (e != cudaSuccess) return e;
+    if (occ < 1) return cudaErrorInvalidConfiguration;
+    // one chunk per warp at most; at most the resident CTAs (each copies the filter)
+    const uint64_t want = (chunks + kSmemThreads / 32 - 1) / (kSmemThreads / 32);
+    const int grid = static_cast<int>(std::max<uint64_t>(1, std::min<uint64_t>(want, static_cast<uint64_t>(sms) * occ)));
+    probe_smem_kernel<Ops><<<grid, kSmemThreads, bytes, s>>>(a, bits, words32);
+    return cudaGetLastError();
+  }
+};
+
+// Probe kernels of one Ops type; Pairs = false leaves the partitioned plan
+// out, Smem = false the shared-memory plan.
+template <class Ops, bool Pairs, bool Smem = false>
 ProbeKernels probe_entry() {
   using F = FusedLaunch<Ops>;
   using B8 = BitsLaunch<Ops, 8>;
@@ -134,7 +167,8 @@ ProbeKernels probe_entry() {
   using P8 = PairsLaunch<Ops, 8>;
   using P4 = PairsLaunch<Ops, 4>;
   ProbeKernels k{&F::run, &F::occupancy, {&B8::run, &B4::run}, {&B8::occupancy, &B4::occupancy},
-                 {nullptr, nullptr}, {nullptr, nullptr}};
+                 {nullptr, nullptr}, {nullptr, nullptr}, nullptr};
+  if constexpr (Smem) k.probe_smem = &SmemLaunch<Ops>::run;
   if constexpr (Pairs) {
     k.probe_pairs[0] = &P8::run;
     k.probe_pairs[1] = &P4::run;
@@ -147,7 +181,7 @@ ProbeKernels probe_entry() {
 template <typename Word, int W, int S, int Z, int K>
 BloomKernels bloom_entry() {
   using C = BloomCfg<Word, W, S, Z, K>;
-  return BloomKernels{static_cast<uint32_t>(sizeof(Word)), W, S, Z, K, probe_entry<BloomOps<C>, true>(),
+  return BloomKernels{static_cast<uint32_t>(sizeof(Word)), W, S, Z, K, probe_entry<BloomOps<C>, true, true>(),
                       &BloomLaunch<C>::build};
 }
 

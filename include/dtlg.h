@@ -168,9 +168,13 @@ dtlg_status dtlg_batch_contains_gather(const dtlg_filter* f, const uint64_t* fil
                                        const uint32_t* col_bytes, void* const* out_cols, uint32_t* match_positions,
                                        uint32_t match_offset, uint64_t* match_cnt_dev, void* workspace,
                                        size_t workspace_bytes, dtlg_stream_t stream);
-/* Probe tuning of one filter (set by the autotuner, dtlg/autotune.py):
+/* Probe tuning of one filter (set by the autotuner, dtlg_autotune_probe):
  * mode 0 = automatic, 1 = one fused kernel (probe + ordered compaction),
- * 2 = two streaming kernels (match bitmask, then compaction); variant selects
+ * 2 = two streaming kernels (match bitmask, then compaction), 3 = partitioned
+ * (keys sorted into L2-sized block ranges; Bloom and blocked cuckoo filters),
+ * 4 = match bitmask against a copy of the filter in every CTA's shared memory
+ * (Bloom and classic Bloom filters of at most 192 KiB); a plan the filter does
+ * not offer falls back to 2.  variant selects
  * the register budget of the bitmask kernel (-1 = automatic, 0 = 32 registers
  * at 8 CTAs/SM, 1 = 64 registers at 4 CTAs/SM).  Results never change.
  * (The reference's counterpart is its per-config SIMD unroll factor,
@@ -194,8 +198,8 @@ dtlg_status dtlg_set_l2_fetch_granularity(int bytes, int* in_effect);
 /* Probe autotuner, the counterpart of the reference's calibrate() tuners
  * (blocked_bloomfilter_tune_impl.hpp:162-268, cuckoofilter_tune_impl.hpp:
  * 118-225), which time SIMD unroll factors: times every probe plan (fused;
- * bitmask kernel x register budget x block-range passes; partitioned for
- * Bloom filters beyond 32 MiB) on these keys, `reps` runs each, keeps the
+ * bitmask kernel x register budget x block-range passes; partitioned beyond
+ * 32 MiB; shared-memory up to 192 KiB) on these keys, `reps` runs each, keeps the
  * fastest on the handle (as dtlg_set_probe_options / _passes would) and
  * reports it.  All plans must agree on the match count (else DTLG_ERR_CUDA).
  * match_positions: device, capacity >= n (scratch). */

@@ -50,7 +50,7 @@ def test_reference_fixtures(cbf_golden):
         got = w.cpu().numpy().view(np.uint32)[: e["size_u32"]]
         assert np.array_equal(got, arr[f"cbf_{e['id']}_words"]), e
         pk, _ = keygen.probe_keys(e["n_build"], e["n_probe"], e["hit_ratio"], e["seed"])
-        for mode in (1, 2, 3):
+        for mode in (1, 2, 3, 4):
             f.set_probe_options(mode, e["id"] % 2)
             f.set_probe_passes(1 + e["id"] % 3)   # ignored: a classic probe is one pass
             assert np.array_equal(gpu_probe(f, w, pk, e["match_offset"], pad=(e["id"] + 1) % 4),
@@ -73,7 +73,7 @@ def test_large_filters_match_oracle():
         assert np.array_equal(words, ref), (m, k, magic)
         pk, _ = keygen.probe_keys(n, 1 << 20, 0.2, 77)
         exp = o.batch_contains(ref, pk, 5)
-        for mode in (1, 2):
+        for mode in (1, 2, 4):   # 4 falls back to 2 above 192 KiB
             f.set_probe_options(mode, -1)
             assert np.array_equal(gpu_probe(f, w, pk, 5), exp), (m, k, magic, mode)
         del w, words, ref

@@ -72,7 +72,7 @@ def test_bloom_every_config_bit_exact():
             pk, _ = keygen.probe_keys(n, 3001, 0.4, seed)
             off = (1 << 32) - 1500 if ci % 2 else 17
             exp = ob.batch_contains(ref_words, pk, off)
-            for mode in (1, 2, 3):  # fused; bitmask (1-3 block-range passes); partitioned
+            for mode in (1, 2, 3, 4):  # fused; bitmask (1-3 block-range passes); partitioned; shared memory
                 f.set_probe_options(mode, ci % 2)
                 f.set_probe_passes(1 + ci % 3)
                 assert np.array_equal(gpu_probe(f, words, pk, off, pad=(ci + 1) % 4), exp), (wb, w, s, z, k, m, mode)
@@ -92,6 +92,32 @@ def test_bloom_golden_vectors(golden):
         assert np.array_equal(gpu_probe(f, words, pk, e["match_offset"]), arr[f"bloom_{e['id']}_hits"]), e
 
 
+def test_shared_memory_plan():
+    """Plan 4 (filter copied into shared memory): available up to 192 KiB,
+    a fallback to plan 2 above, never the automatic choice (plan 2 in one
+    pass: two kernels); always the oracle's match list."""
+    L = F.lib()
+    for (wb, w, s_, z, k) in ((8, 8, 8, 1, 8), (4, 1, 1, 1, 4), (8, 8, 8, 2, 8), (4, 16, 1, 1, 6)):
+        for kib in (4, 64, 96, 160, 256):
+            m = kib * 8192 - 8 * 64 * (kib % 3)  # POW2 and MAGIC sizes
+            ob = O.Bloom(wb, w, s_, z, k, m)
+            f = F.construct(F.blocked_bloomfilter_config(k=k, word_size=wb, word_cnt_per_block=w, sector_cnt=s_,
+                                                         zone_cnt=z), m)
+            n = int(ob.m_actual // 12)
+            bk = keygen.build_keys(n, kib)
+            rw = ob.alloc()
+            ob.insert(rw, bk)
+            words = dev_words(rw)
+            pk, _ = keygen.probe_keys(n, (1 << 21) + 3, 0.1, kib)
+            exp = ob.batch_contains(rw, pk, 77)
+            f.set_probe_options(0, -1)
+            assert L.dtlg_probe_kernel_count(f._h, len(pk)) == 2
+            for mode in (0, 4):
+                f.set_probe_options(mode, -1)
+                for pad in (0, 3):
+                    assert np.array_equal(gpu_probe(f, words, pk, 77, pad), exp), (wb, w, s_, z, k, kib, mode, pad)
+
+
 @pytest.mark.parametrize("n", [0, 1, 2, 3, 4, 5, 31, 1023, 1024, 4095, 4096, 4097, 8191, 65537, 300001])
 def test_probe_lengths_and_alignment(n):
     ob = O.Bloom(8, 8, 8, 1, 8, 3 * (1 << 16))
@@ -103,7 +129,7 @@ def test_probe_lengths_and_alignment(n):
     pk, _ = keygen.probe_keys(20000, n, 0.5, 5)
     exp = ob.batch_contains(rw, pk, 9)
     for mode, variant, passes in ((0, -1, 0), (1, -1, 0), (2, 0, 1), (2, 1, 1), (2, 1, 3), (2, 0, 16), (3, 0, 0),
-                                  (3, 1, 0)):
+                                  (3, 1, 0), (4, -1, 0)):
         f.set_probe_options(mode, variant)
         f.set_probe_passes(passes)
         for pad in range(4):
