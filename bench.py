@@ -70,7 +70,24 @@ def parse():
     ap.add_argument("--probe-mode", type=int, default=0,
                     help="0 auto, 1 fused, 2 bitmask + block-range passes, 3 partitioned, 4 shared-memory filter copy")
     ap.add_argument("--probe-passes", type=int, default=0, help="block-range passes of mode 2 (0 auto)")
-    return ap.parse_args()
+    ap.add_argument("--log2-build", type=int, default=None, help="Bloom workloads: log2 of the build keys")
+    ap.add_argument("--bits-per-key", type=int, default=None, help="Bloom workloads: filter bits per build key")
+    ap.add_argument("--hit-ratio", type=float, default=None, help="Bloom workloads: fraction of member probes")
+    args = ap.parse_args()
+    overrides = (args.log2_build, args.bits_per_key, args.hit_ratio)
+    if any(v is not None for v in overrides):
+        # a variant of a Bloom workload (the shapes of the sectorized config:
+        # n in {2^22, 2^26, 2^28}, 8/12/16 bits per key, 1/10/50 % hits)
+        if args.workload not in WORKLOADS:
+            ap.error("--log2-build / --bits-per-key / --hit-ratio apply to Bloom workloads only")
+        wb, w, s_, z, k, ln, bpk, lp, hit = WORKLOADS[args.workload]
+        ln = ln if args.log2_build is None else args.log2_build
+        bpk = bpk if args.bits_per_key is None else args.bits_per_key
+        hit = hit if args.hit_ratio is None else args.hit_ratio
+        name = f"{args.workload}_n{ln}_b{bpk}_h{round(hit * 100)}"
+        WORKLOADS[name] = (wb, w, s_, z, k, ln, bpk, lp, hit)
+        args.workload = name
+    return args
 
 
 def cuckoo_bits(n, t, b, lf):
