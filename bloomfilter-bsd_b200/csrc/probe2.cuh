@@ -8,7 +8,8 @@
 // 2. compact_kernel: turns the bitmask into the ascending position list.  A
 //    tile is 65536 keys (2048 mask words); the tile offset comes from a
 //    decoupled look-back (bounded waits, as in probe.cuh) over a few thousand
-//    status words.  It moves 1/8 byte per key in and 4 bytes per match out.
+//    status words.  It moves 1/8 byte per key in and 4 bytes per match out,
+//    staged per warp in shared memory so the stores are coalesced.
 // The extra traffic against the fused kernel is the bitmask, 2/8 byte per key.
 #pragma once
 
@@ -116,11 +117,22 @@ probe_smem_kernel(const __grid_constant__ ProbeArgs a, uint32_t* __restrict__ bi
   bits_loop(a, bits, 0, [&](uint32_t key) { return Ops::contains_shared(s_filter, a, key); });
 }
 
+// Ordered compaction.  A tile is kCompactTileWords mask words; warp w of the
+// CTA owns the 256 words w*256 .. w*256+255 of the tile as 8 rows of 32 words
+// (lane l holds word i*32 + l of row i, so every row is one coalesced 128-byte
+// load).  The tile's offset comes from the look-back; the warp's from a CTA
+// scan; each row's from a warp scan.  A row's matches (at most 1024) are
+// first written to a per-warp staging area in shared memory in key order and
+// then stored by the whole warp to consecutive output slots, so the output
+// (and the payload gathers) are coalesced however dense the matches are.
 static __global__ void __launch_bounds__(kCompactThreads) compact_kernel(const __grid_constant__ CompactArgs a) {
   constexpr int kWarps = kCompactThreads / 32;
+  constexpr int kRows = kCompactWordsPerThread;  // rows of 32 words per warp
+  static_assert(kCompactTileWords == kWarps * kRows * 32, "tile = warps x rows x 32 words");
   __shared__ uint32_t s_tile;
   __shared__ uint32_t s_warp[kWarps];
   __shared__ uint32_t s_excl;
+  __shared__ uint32_t s_stage[kWarps][1024];
   const uint32_t lane = threadIdx.x & 31u;
   const uint32_t warp = threadIdx.x >> 5;
   // the look-back helper of probe.cuh reads status / err from a ProbeArgs
@@ -132,27 +144,18 @@ static __global__ void __launch_bounds__(kCompactThreads) compact_kernel(const _
     __syncthreads();
     const uint32_t tile = s_tile;
     if (tile >= a.n_tiles) break;
-    const uint64_t w0 = static_cast<uint64_t>(tile) * kCompactTileWords + threadIdx.x * kCompactWordsPerThread;
-    uint32_t wv[kCompactWordsPerThread];
-    if (w0 + kCompactWordsPerThread <= a.n_words) {
-      const uint4* p = reinterpret_cast<const uint4*>(a.bits + w0);
-      const uint4 x0 = __ldcs(p), x1 = __ldcs(p + 1);
-      wv[0] = x0.x; wv[1] = x0.y; wv[2] = x0.z; wv[3] = x0.w;
-      wv[4] = x1.x; wv[5] = x1.y; wv[6] = x1.z; wv[7] = x1.w;
-    } else {
-#pragma unroll
-      for (int i = 0; i < kCompactWordsPerThread; i++) wv[i] = (w0 + i < a.n_words) ? a.bits[w0 + i] : 0u;
-    }
+    const uint64_t wbase = static_cast<uint64_t>(tile) * kCompactTileWords + static_cast<uint64_t>(warp) * (kRows * 32);
+    uint32_t wv[kRows];
     uint32_t c = 0;
 #pragma unroll
-    for (int i = 0; i < kCompactWordsPerThread; i++) c += __popc(wv[i]);
-    uint32_t incl = c;
-#pragma unroll
-    for (int d = 1; d < 32; d <<= 1) {
-      const uint32_t t = __shfl_up_sync(0xffffffffu, incl, d);
-      if (lane >= static_cast<uint32_t>(d)) incl += t;
+    for (int i = 0; i < kRows; i++) {
+      const uint64_t idx = wbase + static_cast<uint64_t>(i) * 32 + lane;
+      wv[i] = idx < a.n_words ? __ldcs(a.bits + idx) : 0u;
+      c += __popc(wv[i]);
     }
-    if (lane == 31) s_warp[warp] = incl;
+#pragma unroll
+    for (int d = 16; d > 0; d >>= 1) c += __shfl_xor_sync(0xffffffffu, c, d);
+    if (lane == 0) s_warp[warp] = c;  // the warp's match count
     __syncthreads();
     if (warp == 0) {
       const uint32_t v = lane < kWarps ? s_warp[lane] : 0u;
@@ -181,26 +184,45 @@ static __global__ void __launch_bounds__(kCompactThreads) compact_kernel(const _
       }
     }
     __syncthreads();
-    uint32_t pos = s_excl + s_warp[warp] + (incl - c);
-    const uint32_t first = static_cast<uint32_t>(w0 * 32 - a.pre);  // logical index of bit 0 of wv[0]
+    uint32_t pos = s_excl + s_warp[warp];
+    uint32_t* stage = s_stage[warp];
 #pragma unroll
-    for (int i = 0; i < kCompactWordsPerThread; i++) {
+    for (int i = 0; i < kRows; i++) {
+      // the row's matches in key order: lanes in order, bits in order
+      const uint32_t ci = __popc(wv[i]);
+      uint32_t incl = ci;
+#pragma unroll
+      for (int d = 1; d < 32; d <<= 1) {
+        const uint32_t t = __shfl_up_sync(0xffffffffu, incl, d);
+        if (lane >= static_cast<uint32_t>(d)) incl += t;
+      }
+      const uint32_t tot = __shfl_sync(0xffffffffu, incl, 31);
+      if (tot == 0) continue;
+      // logical index of bit 0 of this lane's word
+      const uint32_t first = static_cast<uint32_t>((wbase + static_cast<uint64_t>(i) * 32 + lane) * 32 - a.pre);
       uint32_t m = wv[i];
+      uint32_t o = incl - ci;
       while (m) {
         const uint32_t b = __ffs(m) - 1;
         m &= m - 1;
-        const uint32_t li = first + static_cast<uint32_t>(i) * 32u + b;
-        if (a.out) __stcs(a.out + pos, li + a.match_offset);
+        stage[o++] = first + b;
+      }
+      __syncwarp();
+      for (uint32_t j = lane; j < tot; j += 32) {
+        const uint32_t li = stage[j];
+        if (a.out) __stcs(a.out + pos + j, li + a.match_offset);
         for (uint32_t col = 0; col < a.n_cols; col++) {
           if (a.col_bytes[col] == 8) {
-            __stcs(static_cast<unsigned long long*>(a.out_cols[col]) + pos,
+            __stcs(static_cast<unsigned long long*>(a.out_cols[col]) + pos + j,
                    __ldcs(static_cast<const unsigned long long*>(a.cols[col]) + li));
           } else {
-            __stcs(static_cast<uint32_t*>(a.out_cols[col]) + pos, __ldcs(static_cast<const uint32_t*>(a.cols[col]) + li));
+            __stcs(static_cast<uint32_t*>(a.out_cols[col]) + pos + j,
+                   __ldcs(static_cast<const uint32_t*>(a.cols[col]) + li));
           }
         }
-        pos++;
       }
+      __syncwarp();
+      pos += tot;
     }
     __syncthreads();
   }
