@@ -152,3 +152,43 @@ def test_staged_build_ors_into_existing_words():
     b.run()
     torch.cuda.synchronize()
     assert np.array_equal(data.cpu().numpy().view(np.uint64), rw)
+
+
+def test_batch_with_blocked_cuckoo_and_classic_filters():
+    """Blocked cuckoo and classic Bloom filters join a batch as separate
+    launches (the persistent kernel's menu holds the blocked Bloom layouts):
+    classic words byte-identical to the oracle's, blocked cuckoo words probed
+    by the oracle to the same match list, no false negatives; the Bloom
+    filters of the batch still go through the persistent kernel."""
+    items, checks = [], []
+    specs = [("bloom", 20000), ("bcf", 30000), ("classic", 25000), ("bloom", 5000), ("bcf", 3000)]
+    for i, (kind, nb) in enumerate(specs):
+        bk = keygen.build_keys(nb, 60 + i)
+        pk, _ = keygen.probe_keys(nb, 3 * nb, 0.3, 60 + i)
+        if kind == "bloom":
+            f = F.construct(F.blocked_bloomfilter_config(k=8, word_size=8, word_cnt_per_block=8, sector_cnt=8), nb * 12)
+            o = O.Bloom(8, 8, 8, 1, 8, nb * 12)
+        elif kind == "bcf":
+            f = F.bcf(nb * 32 + 11, 64, 16, 4)
+            o = O.BlockedCuckoo(nb * 32 + 11, 64, 16, 4)
+        else:
+            f = F.bloomfilter_logic(nb * 10, 4)
+            o = O.ClassicBloom(4, nb * 10)
+        items.append(BatchItem(f, f.alloc_filter_data(), dev(bk), dev(pk),
+                               torch.full((len(pk),), -1, dtype=torch.int32, device="cuda"),
+                               torch.full((1,), -1, dtype=torch.int64, device="cuda"), 100 * i))
+        checks.append((kind, o, bk, pk, 100 * i))
+    b = Batch(items, use_graph=False)
+    assert b.fallback_count() == 3
+    b.run()
+    torch.cuda.synchronize()
+    for (kind, o, bk, pk, off), it in zip(checks, items):
+        words = it.filter_data.cpu().numpy().view(np.uint64)
+        if kind != "bcf":
+            ref = o.alloc()
+            o.insert(ref, bk)
+            assert np.array_equal(words, ref), kind
+        assert len(o.batch_contains(words, bk)) == len(bk), kind
+        exp = o.batch_contains(words, pk, off)
+        n = int(it.match_cnt.item())
+        assert n == len(exp) and np.array_equal(it.match_positions[:n].cpu().numpy().view(np.uint32), exp), kind
