@@ -1,6 +1,7 @@
 """The several-GPU plumbing on CPU: two gloo ranks shard a probe (contiguous
 slices, match_offset = slice start, all-gather of counts) and a Bloom build
-(partial filters OR-combined by block range).  The filter work itself is the
+(partial filters OR-combined by block range; also the classic Bloom filter;
+the blocked cuckoo filter is replicated and only its probe shards).  The filter work itself is the
 oracle's (the CPU stand-in for each rank's GPU); what is checked is that the
 sharded results equal the single-process ones."""
 import os
@@ -55,8 +56,27 @@ def _worker(rank, world, port, results):
         dist.all_gather_object(lists, mine.tolist())
         merged = np.concatenate([np.array(x, dtype=np.uint32) for x in lists])
         ref = ob.batch_contains(full, pk, 1000)
+        # classic Bloom filter: OR-combined partial builds equal the full build
+        oc = O.ClassicBloom(5, n * 10 + 3, True)
+        cpart = oc.alloc()
+        oc.insert(cpart, bk[b0:b0 + bn])
+        cwords = torch.from_numpy(cpart.view(np.int64).copy())
+        or_combine(cwords)
+        cfull = oc.alloc()
+        oc.insert(cfull, bk)
+        classic_ok = np.array_equal(cwords.numpy().view(np.uint64), cfull)
+        # blocked cuckoo: no OR-combine (a cuckoo build is not a union), so the
+        # table is built once and replicated; the probe shards as above
+        ox = O.BlockedCuckoo(n * 32, 64, 16, 4)
+        xt = ox.alloc()
+        ox.insert(xt, bk, seed=4)
+        xmine = ox.batch_contains(xt, pk[p0:p0 + pn], p0)
+        xl = [None] * world
+        dist.all_gather_object(xl, xmine.tolist())
+        xmerged = np.concatenate([np.array(x, dtype=np.uint32) for x in xl])
+        bcf_ok = bool(np.array_equal(xmerged, ox.batch_contains(xt, pk, 0)))
         results[rank] = (build_ok, bool(np.array_equal(merged, ref)), total == len(ref),
-                         offs[rank] == int(np.searchsorted(ref, p0 + 1000)))
+                         offs[rank] == int(np.searchsorted(ref, p0 + 1000)), classic_ok, bcf_ok)
     finally:
         dist.destroy_process_group()
 
