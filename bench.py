@@ -50,6 +50,9 @@ BCF_WORKLOADS = {
     # dtl::bcf's default config: 64-byte blocks of 8 buckets x 4 16-bit tags,
     # 256 MiB (DRAM-resident) at half of its slots
     "bcf_dram": (64, 16, 4, 26, 31, 28, 0.10),
+    # the same at 128 MiB (still beyond the 126 MB L2) and 2^26 probes: the
+    # case ncu captures run on
+    "bcf_dram_small": (64, 16, 4, 25, 30, 26, 0.10),
 }
 SEED = 20240601
 
