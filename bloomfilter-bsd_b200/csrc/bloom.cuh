@@ -51,6 +51,15 @@ __device__ __forceinline__ void ld_nc_256(const void* p, unsigned long long& a, 
                : "l"(p));
 }
 
+// The same without allocating the line in L1: for random blocks of a filter
+// that does not fit L1 the allocation only costs L1TEX work (see ProbeArgs::l1na).
+__device__ __forceinline__ void ld_nc_na_256(const void* p, unsigned long long& a, unsigned long long& b,
+                                             unsigned long long& c, unsigned long long& d) {
+  asm volatile("ld.global.nc.L1::no_allocate.v4.u64 {%0,%1,%2,%3}, [%4];"
+               : "=l"(a), "=l"(b), "=l"(c), "=l"(d)
+               : "l"(p));
+}
+
 // Coherent (weak, L1-cacheable) loads for filter words written earlier in the
 // same kernel (the batched build+probe kernel); the .nc path above may only
 // read data that is constant for the whole kernel.
@@ -73,10 +82,11 @@ __device__ __forceinline__ unsigned int ld_weak_32(const void* p) {
 // Loads a whole block of W words with the widest aligned vector loads.  Each
 // load of a random block is one L1 wavefront, so fewer, wider loads raise the
 // probe rate: blocks of >= 32 bytes use 256-bit loads when the filter base is
-// 32-byte aligned (vec32), 128-bit loads otherwise.  NC = false reads through
-// the coherent path (see ld_weak_128).
+// 32-byte aligned (vec32), 128-bit loads otherwise; l1na = the 256-bit loads
+// do not allocate in L1.  NC = false reads through the coherent path (see
+// ld_weak_128).
 template <typename Word, int W, bool NC = true>
-__device__ __forceinline__ void load_block(const Word* base, Word (&v)[W], bool vec32 = false) {
+__device__ __forceinline__ void load_block(const Word* base, Word (&v)[W], bool vec32 = false, bool l1na = false) {
   constexpr int kBytes = W * static_cast<int>(sizeof(Word));
   if constexpr (!NC) {
     if constexpr (kBytes >= 16) {
@@ -97,8 +107,14 @@ __device__ __forceinline__ void load_block(const Word* base, Word (&v)[W], bool 
     if (vec32) {
       unsigned long long* d = reinterpret_cast<unsigned long long*>(&v[0]);
       const unsigned long long* p = reinterpret_cast<const unsigned long long*>(base);
+      if (l1na) {
 #pragma unroll
-      for (int i = 0; i < kBytes / 32; i++) ld_nc_256(p + 4 * i, d[4 * i], d[4 * i + 1], d[4 * i + 2], d[4 * i + 3]);
+        for (int i = 0; i < kBytes / 32; i++)
+          ld_nc_na_256(p + 4 * i, d[4 * i], d[4 * i + 1], d[4 * i + 2], d[4 * i + 3]);
+      } else {
+#pragma unroll
+        for (int i = 0; i < kBytes / 32; i++) ld_nc_256(p + 4 * i, d[4 * i], d[4 * i + 1], d[4 * i + 2], d[4 * i + 3]);
+      }
       return;
     }
   }
@@ -157,16 +173,16 @@ struct BloomOps {
     const uint32_t blk = block_index(key * mul_const(0), a.addr);
     if (a.range_on && (blk < a.blk_lo || blk >= a.blk_hi)) return false;  // another pass's block
     return test_block<true>(static_cast<const Word*>(a.filter) + static_cast<uint64_t>(blk) * kW, key,
-                            a.vec32 != 0);
+                            a.vec32 != 0, a.l1na != 0);
   }
 
   // The key's bits in the block at `base`; NC selects the read-only load path.
   template <bool NC>
-  __device__ __forceinline__ static bool test_block(const Word* base, uint32_t key, bool vec32) {
+  __device__ __forceinline__ static bool test_block(const Word* base, uint32_t key, bool vec32, bool l1na = false) {
     bool ok = true;
     if constexpr (kS.fixed_words) {
       Word v[kW];
-      load_block<Word, kW, NC>(base, v, vec32);
+      load_block<Word, kW, NC>(base, v, vec32, l1na);
       static_for<kS.ng>([&](auto G) {
         constexpr int g = decltype(G)::value;
         const Word m = group_mask<g>(key);
