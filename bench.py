@@ -54,6 +54,12 @@ BCF_WORKLOADS = {
     # case ncu captures run on
     "bcf_dram_small": (64, 16, 4, 25, 30, 26, 0.10),
 }
+CLASSIC_WORKLOADS = {
+    # name: (k, log2 n, bits/key, log2 probes, hit ratio, MAGIC addressing)
+    # the classic Bloom filter (bloomfilter_logic<u32, POW2>): k = 4 random
+    # words per key, 8 MiB (L2-resident)
+    "classic_l2": (4, 22, 16, 28, 0.10, False),
+}
 SEED = 20240601
 
 
@@ -64,7 +70,7 @@ def parse():
     ap.add_argument("--warmup", type=int, default=5)
     ap.add_argument("--impl", choices=("dtlg", "reference"), default="dtlg")
     ap.add_argument("--workload", choices=sorted(WORKLOADS) + sorted(CUCKOO_WORKLOADS) + sorted(BCF_WORKLOADS)
-                    + ["batched512"],
+                    + sorted(CLASSIC_WORKLOADS) + ["batched512"],
                     default="sectorized_dram")
     ap.add_argument("--no-cpu-baseline", action="store_true")
     ap.add_argument("--batch-filters", type=int, default=512, help="batched512: number of filters")
@@ -119,6 +125,15 @@ def bcf_sectors(block_bytes, t, a):
 
 
 def workload_config(name, n_gpus):
+    if name in CLASSIC_WORKLOADS:
+        k, ln, bpk, lp, h, magic = CLASSIC_WORKLOADS[name]
+        return {
+            "workload": name, "filter": f"classic Bloom (bloomfilter_logic) k={k} {'MAGIC' if magic else 'POW2'}",
+            "bits_per_key": bpk, "build_keys": 1 << ln, "probe_keys_per_gpu": 1 << lp,
+            "global_batch": (1 << lp) * n_gpus, "hit_ratio": h, "filter_bytes": (1 << ln) * bpk // 8,
+            "parallelism": f"dp{n_gpus} (replicated filter, sharded probes)",
+            "l2_flush": "inputs larger than L2 (keys 4 B/key x probes + filter words)",
+        }
     if name in BCF_WORKLOADS:
         bb, t, a, ln, lm, lp, h = BCF_WORKLOADS[name]
         return {
@@ -230,7 +245,16 @@ def cpu_reference_probe(words_np, cfg, m, probe_np, threads, budget_s, want_kind
 
     import oracle as O
     out = np.empty(len(probe_np) + 64, dtype=np.uint32)
-    if cfg[0] == "bcf":
+    if cfg[0] == "classic":
+        ref = O.try_refcbf() if want_kind == "reference" else None
+        if ref is None:
+            raise RuntimeError("the reference's bloomfilter_logic is not built (oracle/_ref)")
+        f = ref.create(cfg[1], m, cfg[2])
+        words_u32 = np.zeros(f.size_u32 + 16, dtype=np.uint32)
+        words_u32[: f.size_u32] = words_np.view(np.uint32)[: f.size_u32]
+        kind = "reference"
+        run = lambda keys: f.batch_contains_mt(words_u32, keys, threads, out=out)  # noqa: E731
+    elif cfg[0] == "bcf":
         ref = bcf_reference() if want_kind == "reference" else None
         if ref is None:
             raise RuntimeError("the reference's dtl::bcf is not built (oracle/_ref)")
@@ -304,6 +328,12 @@ def run_dtlg(args):
         m = cuckoo_bits(n_build, tag_bits, slots, lf)
         f = dtlg.cf(m, tag_bits, slots)
         block_bytes, sectors = (tag_bits * slots + 7) // 8, 2   # two buckets, 8-byte aligned: one sector each
+    elif args.workload in CLASSIC_WORKLOADS:
+        ck, ln, bpk, lp, hit, cmagic = CLASSIC_WORKLOADS[args.workload]
+        n_build, P = 1 << ln, 1 << lp
+        m = n_build * bpk
+        f = dtlg.bloomfilter_logic(m, ck, dtlg.MAGIC if cmagic else dtlg.POWER_OF_TWO)
+        sectors = ck   # k words anywhere in the filter: one sector each (members; non-members stop earlier)
     elif args.workload in BCF_WORKLOADS:
         block_bytes, tag_bits, assoc, ln, lm, lp, hit = BCF_WORKLOADS[args.workload]
         n_build, P = 1 << ln, 1 << lp
@@ -460,6 +490,8 @@ def run_dtlg(args):
                 fcfg = ("cuckoo", tag_bits, slots)
             elif args.workload in BCF_WORKLOADS:
                 fcfg = ("bcf", block_bytes, tag_bits, assoc)
+            elif args.workload in CLASSIC_WORKLOADS:
+                fcfg = ("classic", ck, cmagic)
             else:
                 fcfg = (wb, w, s, z, k)
             rate, kind, n, c, variant = cpu_reference_probe(words_np, fcfg, m, probe_np, threads, budget_s=4.0)
@@ -505,7 +537,7 @@ def run_reference(args):
         return
     threads = len(os.sched_getaffinity(0))
     chunk = 1 << 24
-    if args.workload in BCF_WORKLOADS:
+    if args.workload in BCF_WORKLOADS or args.workload in CLASSIC_WORKLOADS:
         run_reference_bcf(args, threads, chunk)
         return
     if args.workload in CUCKOO_WORKLOADS:
@@ -570,21 +602,34 @@ def run_reference(args):
 
 
 def run_reference_bcf(args, threads, chunk):
-    """--impl reference for the blocked cuckoo workloads: the reference's
-    dtl::bcf (bcf.cpp compiled from its sources), built by one thread (its
+    """--impl reference for the blocked cuckoo and classic Bloom workloads: the
+    reference's dtl::bcf (bcf.cpp compiled from its sources) or
+    bloomfilter_logic (its header, instantiated), built by one thread (their
     inserts are not atomic), probed by all host threads."""
     import numpy as np
 
     from dtlg import keygen
     world = int(os.environ.get("WORLD_SIZE", "1"))
-    ref = bcf_reference()
+    if args.workload in CLASSIC_WORKLOADS:
+        sys.path.insert(0, os.path.join(ROOT, "oracle"))
+        import oracle as O
+        ref = O.try_refcbf()
+        what = "oracle/_ref/libdtlref_cbf.so (the reference's bloomfilter_logic)"
+    else:
+        ref = bcf_reference()
+        what = "oracle/_ref/libdtlref_bcf*.so (the reference's dtl::bcf)"
     if ref is None:
-        print(json.dumps({"impl": "reference", "unavailable": "oracle/_ref/libdtlref_bcf*.so (the reference's "
-                                                               "dtl::bcf) is not built on this machine"}))
+        print(json.dumps({"impl": "reference", "unavailable": f"{what} is not built on this machine"}))
         return
-    bb, t, a, ln, lm, lp, hit = BCF_WORKLOADS[args.workload]
+    if args.workload in CLASSIC_WORKLOADS:
+        k, ln, bpk, lp, hit, magic = CLASSIC_WORKLOADS[args.workload]
+        f = ref.create(k, (1 << ln) * bpk, magic)
+        variant, api = "scalar", "bloomfilter_logic batch_contains"
+    else:
+        bb, t, a, ln, lm, lp, hit = BCF_WORKLOADS[args.workload]
+        f = ref.create(1 << lm, bb, t, a)
+        variant, api = ref.variant, "dtl::bcf batch_contains"
     n_build, P = 1 << ln, 1 << lp
-    f = ref.create(1 << lm, bb, t, a)
     words = f.alloc()
     for c0 in range(0, n_build, chunk):
         f.insert(words, keygen.build_keys(min(chunk, n_build - c0), SEED, start=c0))
@@ -613,8 +658,8 @@ def run_reference_bcf(args, threads, chunk):
         "config": workload_config(args.workload, world),
         "cpu_baseline": {"value": round(value, 4), "unit": "Gkeys/s", "cores": threads, "kind": "reference",
                          "sample": f"{n} of the workload's probe keys per step, {threads} threads x 1024-key "
-                                   f"batches (model/benchmark.cpp:123-165), dtl::bcf batch_contains "
-                                   f"({ref.variant} build)", "match_count": int(cnt)},
+                                   f"batches (model/benchmark.cpp:123-165), {api} "
+                                   f"({variant} build)", "match_count": int(cnt)},
         "e2e": {"value": round(value, 4), "unit": "Gkeys/s", "h2d_bytes_per_step": 0, "d2h_bytes_per_step": 0},
     }), flush=True)
 

@@ -295,12 +295,14 @@ dtlg_status launch_probe(const dtlg_filter* f, const uint64_t* words, const uint
     const uint32_t words32 = static_cast<uint32_t>((f->d.m_actual + 31) / 32);
     DTLG_CUDA(f->pk->probe_smem(a, bits, words32, (n_phys + 127) / 128, ds->sms, stream));
   } else if (mode == 2) {
-    // Random blocks of a filter that cannot live in L1 are read without
+    // Random blocks of a Bloom filter that cannot live in L1 are read without
     // allocating in L1 (B200, u64 w=8 s=8 k=8, 2^28 probes: 8 MiB filter
     // 118.5 -> 127.1 Gkeys/s; a 64 KiB L1-resident filter falls from 150.8 to
     // 71.1 without L1 allocation, and the partitioned plan's pair probe from
-    // 76.0 to 72.9, so both keep allocating).
-    a.l1na = (f->d.m_actual / 8) > kL1NoAllocBytes ? 1u : 0u;
+    // 76.0 to 72.9, so both keep allocating).  Not for the other kinds:
+    // cuckoo buckets 75.6 -> 47.9, blocked cuckoo (128 MiB) 102.1 -> 98.9,
+    // classic Bloom unchanged.
+    a.l1na = (f->bk != nullptr && (f->d.m_actual / 8) > kL1NoAllocBytes) ? 1u : 0u;
     // match bitmask, in block-range passes over large filters (each pass
     // probes only the keys whose block lies in its range, so the concurrently
     // touched part of the filter stays within the GPU's address-translation reach)

@@ -134,17 +134,13 @@ struct BcfOps {
   // fetch the second word separately only when it lies in another sector
   // (half the keys in a 64-byte block); a one-word block is read once.
   __device__ __forceinline__ static void load_pair(const Word* p, uint32_t i1, uint32_t i2, uint32_t bb,
-                                                   bool vec32, bool l1na, Word& w1, Word& w2) {
+                                                   bool vec32, Word& w1, Word& w2) {
     constexpr uint32_t kWps = 32u / sizeof(Word);  // words per 32-byte sector
     constexpr uint32_t kLwps = sizeof(Word) == 8 ? 2u : 3u;
     if (vec32 && bb >= kLwps) {
       const uint32_t s1 = i1 >> kLwps;
       unsigned long long v[4];
-      if (l1na) {
-        ld_nc_na_256(p + (s1 << kLwps), v[0], v[1], v[2], v[3]);
-      } else {
-        ld_nc_256(p + (s1 << kLwps), v[0], v[1], v[2], v[3]);
-      }
+      ld_nc_256(p + (s1 << kLwps), v[0], v[1], v[2], v[3]);
       w1 = pick(v, i1 & (kWps - 1u));
       w2 = (i2 >> kLwps) == s1 ? pick(v, i2 & (kWps - 1u)) : __ldg(p + i2);
     } else if (bb == 0) {
@@ -163,7 +159,7 @@ struct BcfOps {
     bucket_tag(hv, a.bcf_bucket_bits, i1, i2, tag);
     const Word* p = static_cast<const Word*>(a.filter) + (static_cast<uint64_t>(blk) << a.bcf_bucket_bits);
     Word w1, w2;
-    load_pair(p, i1, i2, a.bcf_bucket_bits, a.vec32 != 0u, a.l1na != 0u, w1, w2);
+    load_pair(p, i1, i2, a.bcf_bucket_bits, a.vec32 != 0u, w1, w2);
     return (w1 == static_cast<Word>(Cfg::kOverflow)) | (w2 == static_cast<Word>(Cfg::kOverflow)) | has(w1, tag) |
            has(w2, tag);
   }

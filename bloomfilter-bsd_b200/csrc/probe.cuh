@@ -40,8 +40,8 @@ struct ProbeArgs {
   // 1 when the filter base is 32-byte aligned: blocks of >= 32 bytes are then
   // read with 256-bit loads.
   uint32_t vec32;
-  // 1: those 256-bit loads do not allocate in L1 (bitmask plan, filters that
-  // cannot live in L1; set by the planner)
+  // 1: a Bloom filter's 256-bit block loads do not allocate in L1 (bitmask
+  // plan, filters that cannot live in L1; set by the planner)
   uint32_t l1na;
   // blocked cuckoo filter: log2(buckets per block), and the shift that turns
   // the block hash into the bucket hash (32: the bucket hash is key * C[0])

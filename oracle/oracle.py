@@ -544,7 +544,10 @@ def try_refbcf(variant="scalar"):
 
 
 class RefCbf:
-    """The reference's classic Bloom filter (oracle/_ref/libdtlref_cbf.so)."""
+    """The reference's classic Bloom filter (oracle/_ref/libdtlref_cbf.so);
+    its batch_contains has no SIMD path."""
+
+    variant = "scalar"
 
     def __init__(self):
         path = os.path.join(HERE, "_ref", "libdtlref_cbf.so")
