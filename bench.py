@@ -79,6 +79,8 @@ def parse():
     ap.add_argument("--probe-mode", type=int, default=0,
                     help="0 auto, 1 fused, 2 bitmask + block-range passes, 3 partitioned, 4 shared-memory filter copy")
     ap.add_argument("--probe-passes", type=int, default=0, help="block-range passes of mode 2 (0 auto)")
+    ap.add_argument("--build-mode", type=int, default=0,
+                    help="Bloom build plan: 0 auto, 1 one kernel of atomic ORs, 2 keys grouped by block range")
     ap.add_argument("--log2-build", type=int, default=None, help="Bloom workloads: log2 of the build keys")
     ap.add_argument("--bits-per-key", type=int, default=None, help="Bloom workloads: filter bits per build key")
     ap.add_argument("--hit-ratio", type=float, default=None, help="Bloom workloads: fraction of member probes")
@@ -350,9 +352,19 @@ def run_dtlg(args):
         sectors = -(-block_bytes // 32)
     f.set_probe_options(args.probe_mode, -1)
     f.set_probe_passes(args.probe_passes)
+    f.set_build_options(args.build_mode)
     words = f.alloc_filter_data()
     bk = keygen.build_keys_torch(n_build, SEED)
     assert f.batch_insert(words, bk), "build failed"
+    # build throughput (setup, not the metric): a second build into zeroed words
+    torch.cuda.synchronize()
+    words.zero_()
+    b0, b1 = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
+    b0.record()
+    assert f.batch_insert(words, bk), "build failed"
+    b1.record()
+    torch.cuda.synchronize()
+    build_ms = b0.elapsed_time(b1)
     if args.workload in CUCKOO_WORKLOADS:
         occupied = f.count_occupied_slots(words)
         assert occupied == n_build, (occupied, n_build)
@@ -439,6 +451,8 @@ def run_dtlg(args):
         "kernels_per_step": L.dtlg_probe_kernel_count(f._h, P),
         "match_count_per_gpu": count,
         "clocks": clk,
+        "build": {"ms": round(build_ms, 3), "gkeys_s": round(n_build / (build_ms / 1e3) / 1e9, 3),
+                  "api": "dtlg_batch_insert (device keys), second build into zeroed words, not in the metric"},
     }
 
     # end to end through the public host-buffer API (pinned keys in, positions out)

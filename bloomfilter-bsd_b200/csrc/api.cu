@@ -234,6 +234,43 @@ void partition_ranges(const dtlg_filter* f, uint32_t* range_log2, uint32_t* n_ra
   *n_ranges = static_cast<uint32_t>((nb + (1ull << L) - 1) >> L);
 }
 
+// Groups keys_al[pre, n_phys) by filter range: (key, logical position) pairs,
+// range by range, in the workspace's pair area (partitioned probe and build).
+// Grids of resident CTAs only: the tiles are strided over the grid, so a
+// second, partial wave would finish its share late (the scatter's 37 KiB of
+// shared memory allow 6 CTAs per SM, not 8).
+cudaError_t launch_partition(const dtlg_filter* f, const uint32_t* keys_al, uint64_t n_phys, uint32_t pre,
+                             char* wsb, const WsLayout& lay, int sms, cudaStream_t stream, PartArgs* out) {
+  PartArgs pa{};
+  pa.keys_al = keys_al;
+  pa.n_phys = n_phys;
+  pa.pre = pre;
+  pa.addr = f->d.addr;
+  pa.block_mul = mul_const(f->xk ? 1 : 0);
+  partition_ranges(f, &pa.range_log2, &pa.n_ranges);
+  pa.n_tiles = part_tiles(n_phys);
+  pa.counts = reinterpret_cast<uint32_t*>(wsb + lay.counts_off);
+  pa.totals = reinterpret_cast<uint32_t*>(wsb + lay.totals_off);
+  pa.pairs = reinterpret_cast<uint2*>(wsb + lay.pairs_off);
+  static const int hist_occ = [] {
+    int o = 0;
+    return cudaOccupancyMaxActiveBlocksPerMultiprocessor(&o, part_hist_kernel, kPartThreads, 0) == cudaSuccess
+               ? std::max(1, o) : 1;
+  }();
+  static const int scatter_occ = [] {
+    int o = 0;
+    return cudaOccupancyMaxActiveBlocksPerMultiprocessor(&o, part_scatter_kernel, kPartThreads, 0) == cudaSuccess
+               ? std::max(1, o) : 1;
+  }();
+  const int hgrid = static_cast<int>(std::min<uint64_t>(pa.n_tiles, static_cast<uint64_t>(sms) * hist_occ));
+  const int sgrid = static_cast<int>(std::min<uint64_t>(pa.n_tiles, static_cast<uint64_t>(sms) * scatter_occ));
+  part_hist_kernel<<<hgrid, kPartThreads, 0, stream>>>(pa);
+  part_scan_kernel<<<pa.n_ranges, 1024, 0, stream>>>(pa);
+  part_scatter_kernel<<<sgrid, kPartThreads, 0, stream>>>(pa);
+  *out = pa;
+  return cudaGetLastError();
+}
+
 // Payload columns copied along with the match positions (probe -> gather).
 struct GatherSpec {
   uint32_t n_cols;
@@ -322,36 +359,8 @@ dtlg_status launch_probe(const dtlg_filter* f, const uint64_t* words, const uint
   } else {
     // partitioned probe: keys grouped by filter range, probed range by range
     PartArgs pa{};
-    pa.keys_al = a.keys_al;
-    pa.n_phys = n_phys;
-    pa.pre = pre;
-    pa.addr = f->d.addr;
-    pa.block_mul = mul_const(f->xk ? 1 : 0);
-    partition_ranges(f, &pa.range_log2, &pa.n_ranges);
-    pa.n_tiles = part_tiles(n_phys);
-    pa.counts = reinterpret_cast<uint32_t*>(wsb + lay.counts_off);
-    pa.totals = reinterpret_cast<uint32_t*>(wsb + lay.totals_off);
-    pa.pairs = reinterpret_cast<uint2*>(wsb + lay.pairs_off);
     DTLG_CUDA(cudaMemsetAsync(bits, 0, bits_words(n_phys) * 4, stream));
-    // grids of resident CTAs only: the tiles are strided over the grid, so a
-    // second, partial wave would finish its share late (the scatter's 37 KiB
-    // of shared memory allow 6 CTAs per SM, not 8)
-    static const int hist_occ = [] {
-      int o = 0;
-      return cudaOccupancyMaxActiveBlocksPerMultiprocessor(&o, part_hist_kernel, kPartThreads, 0) == cudaSuccess
-                 ? std::max(1, o) : 1;
-    }();
-    static const int scatter_occ = [] {
-      int o = 0;
-      return cudaOccupancyMaxActiveBlocksPerMultiprocessor(&o, part_scatter_kernel, kPartThreads, 0) == cudaSuccess
-                 ? std::max(1, o) : 1;
-    }();
-    const int hgrid = static_cast<int>(std::min<uint64_t>(pa.n_tiles, static_cast<uint64_t>(ds->sms) * hist_occ));
-    const int sgrid = static_cast<int>(std::min<uint64_t>(pa.n_tiles, static_cast<uint64_t>(ds->sms) * scatter_occ));
-    part_hist_kernel<<<hgrid, kPartThreads, 0, stream>>>(pa);
-    part_scan_kernel<<<pa.n_ranges, 1024, 0, stream>>>(pa);
-    part_scatter_kernel<<<sgrid, kPartThreads, 0, stream>>>(pa);
-    DTLG_CUDA(cudaGetLastError());
+    DTLG_CUDA(launch_partition(f, a.keys_al, n_phys, pre, wsb, lay, ds->sms, stream, &pa));
     PairsArgs pr{};
     pr.probe = a;
     pr.pairs = pa.pairs;
@@ -385,6 +394,15 @@ dtlg_status launch_probe(const dtlg_filter* f, const uint64_t* words, const uint
   compact_kernel<<<cgrid, kCompactThreads, 0, stream>>>(c);
   DTLG_CUDA(cudaGetLastError());
   return DTLG_OK;
+}
+
+// Bloom build plan for n keys: 1 = one kernel of global atomic ORs, 2 = keys
+// grouped by L2-sized block range first (the probe's partition).  Automatic:
+// the partitioned build for filters beyond 160 MiB and batches of >= 2^20 keys.
+int bloom_build_plan(const dtlg_filter* f, uint64_t n) {
+  if (f->build_mode == 1 || f->build_mode == 2) return f->build_mode;
+  const uint64_t bytes = (f->d.m_actual + 7) / 8;
+  return (n >= kTwoPassMinKeys && bytes > (160ull << 20)) ? 2 : 1;
 }
 
 int grid_for(uint64_t items, int sms) {
@@ -600,13 +618,37 @@ dtlg_status dtlg_batch_insert(const dtlg_filter* f, uint64_t* words, const uint3
     DTLG_CUDA(f->xk->insert(b, grid_for(b.n_phys, ds->sms), stream));
     return DTLG_OK;
   }
+  const uint64_t n_phys = static_cast<uint64_t>(n) + pre;
+  if (bloom_build_plan(f, n) == 2) {
+    // keys grouped by L2-sized block range first (the probe's partition), then
+    // inserted range by range: the atomic ORs hit lines that sit in L2
+    const WsLayout lay = ws_layout(n_phys);
+    void* ws = nullptr;
+    if (cudaMallocFromPoolAsync(&ws, lay.total, ds->pool, stream) != cudaSuccess) return DTLG_ERR_ALLOC;
+    PartArgs pa{};
+    cudaError_t e = launch_partition(f, keys - pre, n_phys, pre, static_cast<char*>(ws), lay, ds->sms, stream, &pa);
+    if (e == cudaSuccess) {
+      const uint64_t vec = (static_cast<uint64_t>(n) + 1) / 2;
+      e = f->bk->build_pairs(pa.pairs, n, words, f->d.addr, grid_for(vec, ds->sms), stream);
+    }
+    cudaFreeAsync(ws, stream);
+    DTLG_CUDA(e);
+    return DTLG_OK;
+  }
   BuildArgs a{};
   a.filter = words;
   a.keys_al = keys - pre;
-  a.n_phys = static_cast<uint64_t>(n) + pre;
+  a.n_phys = n_phys;
   a.pre = pre;
   a.addr = f->d.addr;
   DTLG_CUDA(f->bk->build(a, grid_for((a.n_phys + 3) / 4, ds->sms), stream));
+  return DTLG_OK;
+}
+
+dtlg_status dtlg_set_build_options(dtlg_filter* f, int mode) {
+  if (!f) return DTLG_ERR_NULL;
+  if (mode < 0 || mode > 2) return DTLG_ERR_INVALID_CONFIG;
+  f->build_mode = mode;
   return DTLG_OK;
 }
 

@@ -268,6 +268,22 @@ __global__ void __launch_bounds__(256) bloom_build_kernel(const __grid_constant_
   }
 }
 
+// batch_insert of range-grouped (key, position) pairs (probe3.cuh's
+// partition): consecutive keys hit the same L2-sized block range, so the
+// atomic ORs of a filter far larger than L2 update lines that sit in L2.
+template <class Cfg>
+__global__ void __launch_bounds__(256) bloom_build_pairs_kernel(const uint2* __restrict__ pairs, uint64_t n_pairs,
+                                                                void* filter, const Addr addr) {
+  const uint4* p4 = reinterpret_cast<const uint4*>(pairs);
+  const uint64_t n2 = (n_pairs + 1) >> 1;  // two pairs per 16-byte vector
+  for (uint64_t i = blockIdx.x * static_cast<uint64_t>(blockDim.x) + threadIdx.x; i < n2;
+       i += static_cast<uint64_t>(gridDim.x) * blockDim.x) {
+    const uint4 x = __ldcs(p4 + i);
+    BloomOps<Cfg>::insert(filter, x.x, addr);
+    if (2 * i + 1 < n_pairs) BloomOps<Cfg>::insert(filter, x.z, addr);
+  }
+}
+
 #endif  // __CUDACC__
 
 }  // namespace dtlg

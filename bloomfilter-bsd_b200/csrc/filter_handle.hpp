@@ -18,6 +18,9 @@ struct dtlg_filter {
   int probe_mode = 0;
   int bits_variant = -1;
   int probe_passes = 0;  // block-range passes of the two-pass probe; 0 = auto
+  // Bloom build plan (dtlg_set_build_options): 0 = auto, 1 = one kernel of
+  // global atomic ORs, 2 = keys grouped by block range first
+  int build_mode = 0;
 };
 
 namespace dtlg {

@@ -45,6 +45,9 @@ struct BloomKernels {
   uint32_t word_bytes, w, s, z, k;
   ProbeKernels pk;
   build_fn build;
+  // build from range-grouped (key, position) pairs
+  cudaError_t (*build_pairs)(const uint2* pairs, uint64_t n_pairs, void* filter, const Addr& addr, int grid,
+                             cudaStream_t);
 };
 
 struct CuckooKernels {
@@ -129,6 +132,11 @@ struct BloomLaunch {
     bloom_build_kernel<Cfg><<<grid, 256, 0, s>>>(a);
     return cudaGetLastError();
   }
+  static cudaError_t build_pairs(const uint2* pairs, uint64_t n_pairs, void* filter, const Addr& addr, int grid,
+                                 cudaStream_t s) {
+    bloom_build_pairs_kernel<Cfg><<<grid, 256, 0, s>>>(pairs, n_pairs, filter, addr);
+    return cudaGetLastError();
+  }
 };
 
 template <class Ops>
@@ -182,7 +190,7 @@ template <typename Word, int W, int S, int Z, int K>
 BloomKernels bloom_entry() {
   using C = BloomCfg<Word, W, S, Z, K>;
   return BloomKernels{static_cast<uint32_t>(sizeof(Word)), W, S, Z, K, probe_entry<BloomOps<C>, true, true>(),
-                      &BloomLaunch<C>::build};
+                      &BloomLaunch<C>::build, &BloomLaunch<C>::build_pairs};
 }
 
 template <int T, int B>

@@ -105,6 +105,7 @@ SIGNATURES = {
     "dtlg_batch_contains_noalloc": (_i, [_vp, _vp, _vp, _u32, _vp, _u32, _vp, _vp]),
     "dtlg_set_probe_options": (_i, [_vp, _i, _i]),
     "dtlg_set_probe_passes": (_i, [_vp, _i]),
+    "dtlg_set_build_options": (_i, [_vp, _i]),
     "dtlg_probe_kernel_count": (_i, [_vp, _u32]),
     "dtlg_set_l2_fetch_granularity": (_i, [_i, C.POINTER(_i)]),
     "dtlg_autotune_probe": (_i, [_vp, _vp, _vp, _u32, _vp, _i, _vp, C.POINTER(ProbePlanS)]),

@@ -124,6 +124,11 @@ class filter_base:  # noqa: N801 (reference name)
         """Block-range passes of the two-kernel probe (0 = automatic)."""
         check(lib().dtlg_set_probe_passes(self._h, int(passes)), "set_probe_passes")
 
+    def set_build_options(self, mode=0):
+        """Bloom build plan: 0 automatic, 1 one kernel of global atomic ORs,
+        2 keys grouped by L2-sized block range first (same words)."""
+        check(lib().dtlg_set_build_options(self._h, int(mode)), "set_build_options")
+
     def autotune(self, filter_data, keys, reps=5):
         """Times every probe plan on these keys and keeps the fastest for this
         filter (the reference's calibrate(), blocked_bloomfilter_tune_impl.hpp:

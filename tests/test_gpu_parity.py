@@ -69,6 +69,12 @@ def test_bloom_every_config_bit_exact():
             assert f.batch_insert(words, dev_keys(bk, pad=ci % 4))
             got = words.cpu().numpy().view(np.uint64)
             assert np.array_equal(got, ref_words), (wb, w, s, z, k, m)
+            # the partitioned build plan: the same words
+            f.set_build_options(2)
+            words2 = f.alloc_filter_data()
+            assert f.batch_insert(words2, dev_keys(bk, pad=(ci + 2) % 4))
+            assert np.array_equal(words2.cpu().numpy().view(np.uint64), ref_words), (wb, w, s, z, k, m, "plan 2")
+            f.set_build_options(0)
             pk, _ = keygen.probe_keys(n, 3001, 0.4, seed)
             off = (1 << 32) - 1500 if ci % 2 else 17
             exp = ob.batch_contains(ref_words, pk, off)
@@ -246,3 +252,27 @@ def test_large_filter_property():
     exp = ob.batch_contains(rw, pk)
     assert np.array_equal(got, exp)
     assert np.all(np.isin(np.nonzero(member)[0].astype(np.uint32), got))
+
+
+def test_partitioned_build_large_filter():
+    """Filters beyond 160 MiB are built through the partition automatically:
+    the same words as the one-kernel build (and, on a sample, the oracle's
+    probe of them), for a sectorized and a zoned layout, POW2 and MAGIC."""
+    for (wb, w, s_, z, k), m in (((8, 8, 8, 1, 8), 1 << 31), ((8, 8, 8, 2, 8), (3 << 29) + 4096)):
+        f = F.construct(F.blocked_bloomfilter_config(k=k, word_size=wb, word_cnt_per_block=w, sector_cnt=s_,
+                                                     zone_cnt=z), m)
+        n = 1 << 25
+        bk = keygen.build_keys_torch(n, 91)
+        auto = f.alloc_filter_data()
+        assert f.batch_insert(auto, bk)
+        f.set_build_options(1)
+        direct = f.alloc_filter_data()
+        assert f.batch_insert(direct, bk)
+        f.set_build_options(0)
+        assert torch.equal(auto, direct), (wb, w, s_, z, k, m)
+        ob = O.Bloom(wb, w, s_, z, k, m)
+        words = auto.cpu().numpy().view(np.uint64)
+        sample = bk[: 1 << 16].cpu().numpy().view(np.uint32)
+        assert len(ob.batch_contains(words, sample)) == len(sample)
+        del auto, direct
+        torch.cuda.empty_cache()
