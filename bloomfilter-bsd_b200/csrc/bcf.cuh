@@ -228,36 +228,50 @@ __device__ __forceinline__ uint32_t bcf_insert_tag(typename Cfg::word_t* w, uint
   return kBcfOverflowed;
 }
 
-// blocked_cuckoofilter_logic.hpp:73-95 with block_logic.hpp:96-118, one key
-// per thread.
+// blocked_cuckoofilter_logic.hpp:73-95 with block_logic.hpp:96-118 for one
+// key; idx seeds the key's kick-slot generator.
 template <class Cfg>
-__global__ void __launch_bounds__(256) bcf_insert_kernel(const __grid_constant__ BcfBuildArgs a) {
+__device__ __forceinline__ void bcf_insert_key(const BcfBuildArgs& a, uint32_t key, uint64_t idx) {
   using Word = typename Cfg::word_t;
   using Ops = BcfOps<Cfg>;
   const uint32_t bb = a.bucket_bits;
+  uint32_t hv, i1, i2, tag;
+  const uint32_t blk = Ops::block_hash(key, a.addr, a.hash_shift, hv);
+  Ops::bucket_tag(hv, bb, i1, i2, tag);
+  Word* block = static_cast<Word*>(a.filter) + (static_cast<uint64_t>(blk) << bb);
+  uint64_t rng = a.seed ^ (0x9E3779B97F4A7C15ull * (idx + 1));
+  uint32_t old = bcf_insert_tag<Cfg>(block + i1, tag, false, rng);
+  if (old == kBcfPlaced || old == kBcfOverflowed) return;
+  uint32_t cur = i2, cur_tag = tag;
+  for (uint32_t c = 0; c < kBcfRelocations; c++) {
+    old = bcf_insert_tag<Cfg>(block + cur, cur_tag, true, rng);
+    if (old == kBcfPlaced || old == kBcfOverflowed) return;
+    cur_tag = old;
+    cur = Ops::alt(cur, cur_tag, bb);
+  }
+  atomicExch(block + cur, static_cast<Word>(Cfg::kOverflow));  // mark_overflow
+}
+
+// One key per thread.
+template <class Cfg>
+__global__ void __launch_bounds__(256) bcf_insert_kernel(const __grid_constant__ BcfBuildArgs a) {
   for (uint64_t p = blockIdx.x * static_cast<uint64_t>(blockDim.x) + threadIdx.x; p < a.n_phys;
        p += static_cast<uint64_t>(gridDim.x) * blockDim.x) {
     if (p < a.pre) continue;
-    const uint32_t key = __ldg(a.keys_al + p);
-    uint32_t hv, i1, i2, tag;
-    const uint32_t blk = Ops::block_hash(key, a.addr, a.hash_shift, hv);
-    Ops::bucket_tag(hv, bb, i1, i2, tag);
-    Word* block = static_cast<Word*>(a.filter) + (static_cast<uint64_t>(blk) << bb);
-    uint64_t rng = a.seed ^ (0x9E3779B97F4A7C15ull * (p + 1));
-    uint32_t old = bcf_insert_tag<Cfg>(block + i1, tag, false, rng);
-    if (old == kBcfPlaced || old == kBcfOverflowed) continue;
-    uint32_t cur = i2, cur_tag = tag;
-    bool placed = false;
-    for (uint32_t c = 0; c < kBcfRelocations; c++) {
-      old = bcf_insert_tag<Cfg>(block + cur, cur_tag, true, rng);
-      if (old == kBcfPlaced || old == kBcfOverflowed) {
-        placed = true;
-        break;
-      }
-      cur_tag = old;
-      cur = Ops::alt(cur, cur_tag, bb);
-    }
-    if (!placed) atomicExch(block + cur, static_cast<Word>(Cfg::kOverflow));  // mark_overflow
+    bcf_insert_key<Cfg>(a, __ldg(a.keys_al + p), p);
+  }
+}
+
+// The same over range-grouped (key, position) pairs (probe3.cuh's
+// partition): consecutive keys hit the same L2-sized block range, so the
+// compare-and-swap steps of a filter far larger than L2 work on lines in L2.
+template <class Cfg>
+__global__ void __launch_bounds__(256) bcf_insert_pairs_kernel(const __grid_constant__ BcfBuildArgs a,
+                                                               const uint2* __restrict__ pairs, uint64_t n_pairs) {
+  for (uint64_t p = blockIdx.x * static_cast<uint64_t>(blockDim.x) + threadIdx.x; p < n_pairs;
+       p += static_cast<uint64_t>(gridDim.x) * blockDim.x) {
+    const uint2 x = __ldcs(pairs + p);
+    bcf_insert_key<Cfg>(a, x.x, x.y);
   }
 }
 

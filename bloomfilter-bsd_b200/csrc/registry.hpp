@@ -65,6 +65,8 @@ struct BcfKernels {
   uint32_t t, a;
   ProbeKernels pk;
   cudaError_t (*insert)(const BcfBuildArgs&, int grid, cudaStream_t);
+  // insert from range-grouped (key, position) pairs
+  cudaError_t (*insert_pairs)(const BcfBuildArgs&, const uint2* pairs, uint64_t n_pairs, int grid, cudaStream_t);
 };
 
 struct ClassicKernels {
@@ -226,11 +228,17 @@ struct BcfLaunch {
     bcf_insert_kernel<BcfCfg<T, A>><<<grid, 256, 0, s>>>(a);
     return cudaGetLastError();
   }
+  static cudaError_t insert_pairs(const BcfBuildArgs& a, const uint2* pairs, uint64_t n_pairs, int grid,
+                                  cudaStream_t s) {
+    bcf_insert_pairs_kernel<BcfCfg<T, A>><<<grid, 256, 0, s>>>(a, pairs, n_pairs);
+    return cudaGetLastError();
+  }
 };
 
 template <int T, int A>
 BcfKernels bcf_entry() {
-  return BcfKernels{T, A, probe_entry<BcfOps<BcfCfg<T, A>>, true>(), &BcfLaunch<T, A>::insert};
+  return BcfKernels{T, A, probe_entry<BcfOps<BcfCfg<T, A>>, true>(), &BcfLaunch<T, A>::insert,
+                    &BcfLaunch<T, A>::insert_pairs};
 }
 #endif
 

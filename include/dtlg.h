@@ -180,13 +180,14 @@ dtlg_status dtlg_batch_contains_gather(const dtlg_filter* f, const uint64_t* fil
  * (The reference's counterpart is its per-config SIMD unroll factor,
  * blocked_bloomfilter_tune.hpp:21-56.) */
 dtlg_status dtlg_set_probe_options(dtlg_filter* f, int mode, int variant);
-/* Build plan of a blocked Bloom filter (no counterpart in the reference, whose
- * batch_insert is one loop): 0 = automatic (2 for filters beyond 160 MiB and
- * batches of >= 2^20 keys, else 1), 1 = one kernel of global atomic ORs,
- * 2 = keys first grouped by L2-sized block range (the partitioned probe's
- * partition, workspace from the library's stream-ordered pool), then inserted
- * range by range so the atomic ORs hit L2.  The filter words are the same
- * under every plan; other filter kinds ignore it. */
+/* Build plan of a blocked Bloom or blocked cuckoo filter (no counterpart in
+ * the reference, whose batch_insert is one loop): 0 = automatic (2 for Bloom
+ * filters beyond 160 MiB and batches of >= 2^20 keys, else 1), 1 = one kernel of
+ * global atomics, 2 = keys first grouped by L2-sized block range (the
+ * partitioned probe's partition, workspace from the library's stream-ordered
+ * pool), then inserted range by range so the atomics hit L2.  Bloom filter
+ * words are the same under every plan; blocked cuckoo builds are randomised
+ * under both (as the reference's); other filter kinds ignore it. */
 dtlg_status dtlg_set_build_options(dtlg_filter* f, int mode);
 /* Block-range passes of the two-kernel probe (0 = automatic, 1..16).  Random
  * probes over more than ~256 MiB of filter exceed the GPU's address-translation

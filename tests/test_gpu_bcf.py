@@ -198,3 +198,38 @@ def test_large_partitioned_probe():
     assert np.array_equal(res[3][res[3] < (1 << 18)].view(np.uint32), exp)
     f.set_probe_options(3, -1)
     assert f.batch_contains(w, bk, n, out, 0) == n
+
+
+def test_partitioned_build():
+    """Build plan 2 (keys grouped by block range first, on request): the same
+    invariants as the one-kernel build, and a false positive rate like it."""
+    for bb, (t, a) in [(64, (16, 4)), (512, (10, 6)), (8, (8, 4)), (128, (12, 4))]:
+        m = (1 << 22) + 4096 * (bb % 3)
+        o = O.BlockedCuckoo(m, bb, t, a)
+        f = F.bcf(m, bb, t, a)
+        n = int((o.m_actual // (t * a)) * a * 0.8)
+        bk = keygen.build_keys(n, 51)
+        f.set_build_options(2)
+        w = f.alloc_filter_data()
+        assert f.batch_insert(w, dev_keys(bk, pad=1))
+        words = host64(w)
+        assert len(o.batch_contains(words, bk)) == n, (bb, t, a)
+        pk, _ = keygen.probe_keys(n, 20000, 0.2, 51)
+        assert np.array_equal(gpu_probe(f, w, pk, 9), o.batch_contains(words, pk, 9)), (bb, t, a)
+    # 256 MiB: plan 2 against plan 1
+    m = 1 << 31
+    f = F.bcf(m, 64, 16, 4)
+    n = 1 << 25
+    bk = keygen.build_keys_torch(n, 52)
+    neg = keygen.build_keys_torch(1 << 22, 52, start=n)
+    out = torch.empty(max(n, 1 << 22), dtype=torch.int32, device="cuda")
+    fps = []
+    for mode in (2, 1):
+        f.set_build_options(mode)
+        w = f.alloc_filter_data()
+        assert f.batch_insert(w, bk)
+        assert f.batch_contains(w, bk, n, out, 0) == n
+        fps.append(f.batch_contains(w, neg, neg.numel(), out, 0))
+        del w
+        torch.cuda.empty_cache()
+    assert abs(fps[0] - fps[1]) <= 0.25 * fps[1] + 5 * np.sqrt(fps[1] + 1), fps
