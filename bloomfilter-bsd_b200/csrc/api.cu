@@ -623,13 +623,16 @@ dtlg_status dtlg_batch_insert(const dtlg_filter* f, uint64_t* words, const uint3
       // keys grouped by L2-sized block range first, as for Bloom filters
       const WsLayout lay = ws_layout(b.n_phys);
       void* ws = nullptr;
-      if (cudaMallocFromPoolAsync(&ws, lay.total, ds->pool, stream) != cudaSuccess) return DTLG_ERR_ALLOC;
-      PartArgs pa{};
-      cudaError_t e = launch_partition(f, b.keys_al, b.n_phys, pre, static_cast<char*>(ws), lay, ds->sms, stream, &pa);
-      if (e == cudaSuccess) e = f->xk->insert_pairs(b, pa.pairs, n, grid_for(n, ds->sms), stream);
-      cudaFreeAsync(ws, stream);
-      DTLG_CUDA(e);
-      return DTLG_OK;
+      if (cudaMallocFromPoolAsync(&ws, lay.total, ds->pool, stream) == cudaSuccess) {
+        PartArgs pa{};
+        cudaError_t e =
+            launch_partition(f, b.keys_al, b.n_phys, pre, static_cast<char*>(ws), lay, ds->sms, stream, &pa);
+        if (e == cudaSuccess) e = f->xk->insert_pairs(b, pa.pairs, n, grid_for(n, ds->sms), stream);
+        cudaFreeAsync(ws, stream);
+        DTLG_CUDA(e);
+        return DTLG_OK;
+      }
+      cudaGetLastError();  // no room for the partition: the one-kernel build
     }
     DTLG_CUDA(f->xk->insert(b, grid_for(b.n_phys, ds->sms), stream));
     return DTLG_OK;
@@ -640,16 +643,20 @@ dtlg_status dtlg_batch_insert(const dtlg_filter* f, uint64_t* words, const uint3
     // inserted range by range: the atomic ORs hit lines that sit in L2
     const WsLayout lay = ws_layout(n_phys);
     void* ws = nullptr;
-    if (cudaMallocFromPoolAsync(&ws, lay.total, ds->pool, stream) != cudaSuccess) return DTLG_ERR_ALLOC;
-    PartArgs pa{};
-    cudaError_t e = launch_partition(f, keys - pre, n_phys, pre, static_cast<char*>(ws), lay, ds->sms, stream, &pa);
-    if (e == cudaSuccess) {
-      const uint64_t vec = (static_cast<uint64_t>(n) + 1) / 2;
-      e = f->bk->build_pairs(pa.pairs, n, words, f->d.addr, grid_for(vec, ds->sms), stream);
+    if (cudaMallocFromPoolAsync(&ws, lay.total, ds->pool, stream) == cudaSuccess) {
+      PartArgs pa{};
+      cudaError_t e = launch_partition(f, keys - pre, n_phys, pre, static_cast<char*>(ws), lay, ds->sms, stream, &pa);
+      if (e == cudaSuccess) {
+        const uint64_t vec = (static_cast<uint64_t>(n) + 1) / 2;
+        e = f->bk->build_pairs(pa.pairs, n, words, f->d.addr, grid_for(vec, ds->sms), stream);
+      }
+      cudaFreeAsync(ws, stream);
+      DTLG_CUDA(e);
+      return DTLG_OK;
     }
-    cudaFreeAsync(ws, stream);
-    DTLG_CUDA(e);
-    return DTLG_OK;
+    // no room for the partition's 8 bytes per key: the one-kernel build
+    // needs no workspace (same words)
+    cudaGetLastError();
   }
   BuildArgs a{};
   a.filter = words;

@@ -184,8 +184,9 @@ dtlg_status dtlg_set_probe_options(dtlg_filter* f, int mode, int variant);
  * the reference, whose batch_insert is one loop): 0 = automatic (2 for Bloom
  * filters beyond 160 MiB and batches of >= 2^20 keys, else 1), 1 = one kernel of
  * global atomics, 2 = keys first grouped by L2-sized block range (the
- * partitioned probe's partition, workspace from the library's stream-ordered
- * pool), then inserted range by range so the atomics hit L2.  Bloom filter
+ * partitioned probe's partition, 8 bytes per key of workspace from the
+ * library's stream-ordered pool; without room there, plan 1), then inserted
+ * range by range so the atomics hit L2.  Bloom filter
  * words are the same under every plan; blocked cuckoo builds are randomised
  * under both (as the reference's); other filter kinds ignore it. */
 dtlg_status dtlg_set_build_options(dtlg_filter* f, int mode);
