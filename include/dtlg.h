@@ -214,7 +214,7 @@ dtlg_status dtlg_set_l2_fetch_granularity(int bytes, int* in_effect);
  * reports it.  All plans must agree on the match count (else DTLG_ERR_CUDA).
  * match_positions: device, capacity >= n (scratch). */
 typedef struct dtlg_probe_plan {
-  int mode;                      /* 1 fused, 2 bitmask + compaction, 3 partitioned */
+  int mode;                      /* 1 fused, 2 bitmask + compaction, 3 partitioned, 4 shared memory */
   int variant;                   /* bitmask kernel register budget (-1: n/a) */
   int passes;                    /* block-range passes of mode 2 (0: automatic) */
   float ms;                      /* median time of one probe of the n keys */
