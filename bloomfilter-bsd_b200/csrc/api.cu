@@ -205,6 +205,16 @@ constexpr uint64_t kSmemMaxBytes = 192ull << 10;
 // 112 Gkeys/s; not allocating, 1-8 MiB: 128.7).
 constexpr uint64_t kL1NoAllocBytes = 256ull << 10;
 
+// Zoned filters of 160-320 MiB read 2-4 words per key: there the bitmask
+// plan in its block-range passes with the 32-register variant beats the
+// partitioned plan (B200, 2^27 probes, 192 / 256 MiB: z=2 u32 110.1 / 89.7 vs
+// 74.4 / 75.3 Gkeys/s, z=4 u64 75.3 / 74.5 vs 67.3 / 68.7, z=2 u64 84.3 vs
+// 76.2 at 256 MiB); from 384 MiB on, the partition wins (73.7 vs 68.1, z=2 u64).
+bool zoned_band(const dtlg_filter* f) {
+  const uint64_t fbytes = (f->d.m_actual + 7) / 8;
+  return f->d.kind == Kind::kZoned && fbytes > (160ull << 20) && fbytes <= (320ull << 20);
+}
+
 int probe_plan(const dtlg_filter* f, uint64_t n) {
   int mode = f->probe_mode;
   const bool partitioned = f->pk->probe_pairs[0] != nullptr;
@@ -215,11 +225,20 @@ int probe_plan(const dtlg_filter* f, uint64_t n) {
   if (mode == 0) {
     if (n < kTwoPassMinKeys) {
       mode = 1;
+    } else if (zoned_band(f)) {
+      mode = 2;
     } else {
       mode = (partitioned && fbytes > (160ull << 20)) ? 3 : 2;
     }
   }
   return mode;
+}
+
+// Register-budget variant of the bitmask / pair kernels: the caller's, else 0
+// in the zoned band, else 1.
+int probe_variant(const dtlg_filter* f) {
+  if (f->bits_variant >= 0 && f->bits_variant < kBitsVariants) return f->bits_variant;
+  return zoned_band(f) ? 0 : 1;
 }
 
 // Ranges of the partitioned probe: 2^L blocks each, about 32 MiB of filter
@@ -325,7 +344,7 @@ dtlg_status launch_probe(const dtlg_filter* f, const uint64_t* words, const uint
     return DTLG_OK;
   }
   uint32_t* bits = reinterpret_cast<uint32_t*>(wsb + lay.bits_off);
-  const int v = (f->bits_variant >= 0 && f->bits_variant < kBitsVariants) ? f->bits_variant : 1;
+  const int v = probe_variant(f);
   a.vec32 = (reinterpret_cast<uintptr_t>(words) & 31u) == 0 ? 1u : 0u;
   if (mode == 4) {
     // the whole filter in every CTA's shared memory
