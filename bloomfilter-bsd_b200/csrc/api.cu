@@ -205,14 +205,24 @@ constexpr uint64_t kSmemMaxBytes = 192ull << 10;
 // 112 Gkeys/s; not allocating, 1-8 MiB: 128.7).
 constexpr uint64_t kL1NoAllocBytes = 256ull << 10;
 
-// Zoned filters of 160-320 MiB read 2-4 words per key: there the bitmask
-// plan in its block-range passes with the 32-register variant beats the
-// partitioned plan (B200, 2^27 probes, 192 / 256 MiB: z=2 u32 110.1 / 89.7 vs
-// 74.4 / 75.3 Gkeys/s, z=4 u64 75.3 / 74.5 vs 67.3 / 68.7, z=2 u64 84.3 vs
-// 76.2 at 256 MiB); from 384 MiB on, the partition wins (73.7 vs 68.1, z=2 u64).
-bool zoned_band(const dtlg_filter* f) {
+// Blocked Bloom filters just beyond the single-pass limit (160-240 MiB; zoned
+// ones, reading 2-4 words per key, up to 320 MiB): the bitmask plan in its
+// block-range passes with the 32-register variant beats the partitioned plan.
+// B200, 2^27 probes, Gkeys/s, bitmask vs partition:
+//   u64 w=8 s=8 k=8     168 / 192 / 224 MiB: 84.9 / 82.7 / 78.2 vs 74.3 / 74.1 / 75.1
+//   u32 w=1 k=4         168 / 192 MiB: 136.2 / 119.5 vs 102.7 / 104.1 (224: even)
+//   u32 w=16 s=1 k=4    168 / 192 / 224 MiB: 97.3 / 91.5 / 84.9 vs 67.5 / 66.6 / 65.2
+//   zoned u32 w=16 z=2  192 / 256 MiB: 110.1 / 89.7 vs 74.4 / 75.3
+//   zoned u64 w=8 z=4   192 / 256 MiB: 75.3 / 74.5 vs 67.3 / 68.7
+// but not for 32-byte blocks (u64 w=4 s=4 k=8, 168 MiB: 83.9 vs 89.7), nor
+// from 384 MiB on (zoned u64 w=8 z=2: 68.1 vs 73.7).
+bool bitmask_band(const dtlg_filter* f) {
+  if (f->d.kind != Kind::kBloom && f->d.kind != Kind::kZoned) return false;
   const uint64_t fbytes = (f->d.m_actual + 7) / 8;
-  return f->d.kind == Kind::kZoned && fbytes > (160ull << 20) && fbytes <= (320ull << 20);
+  const uint64_t block_bytes = static_cast<uint64_t>(f->d.w) * f->d.word_bytes;
+  if (fbytes <= (160ull << 20)) return false;
+  if (f->d.kind == Kind::kZoned) return fbytes <= (320ull << 20);
+  return fbytes <= (240ull << 20) && block_bytes != 32;  // 224 MiB requests round up under MAGIC
 }
 
 int probe_plan(const dtlg_filter* f, uint64_t n) {
@@ -225,7 +235,7 @@ int probe_plan(const dtlg_filter* f, uint64_t n) {
   if (mode == 0) {
     if (n < kTwoPassMinKeys) {
       mode = 1;
-    } else if (zoned_band(f)) {
+    } else if (bitmask_band(f)) {
       mode = 2;
     } else {
       mode = (partitioned && fbytes > (160ull << 20)) ? 3 : 2;
@@ -235,10 +245,10 @@ int probe_plan(const dtlg_filter* f, uint64_t n) {
 }
 
 // Register-budget variant of the bitmask / pair kernels: the caller's, else 0
-// in the zoned band, else 1.
+// in the band above, else 1.
 int probe_variant(const dtlg_filter* f) {
   if (f->bits_variant >= 0 && f->bits_variant < kBitsVariants) return f->bits_variant;
-  return zoned_band(f) ? 0 : 1;
+  return bitmask_band(f) ? 0 : 1;
 }
 
 // Ranges of the partitioned probe: 2^L blocks each, about 32 MiB of filter
