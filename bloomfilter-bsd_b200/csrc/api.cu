@@ -205,24 +205,29 @@ constexpr uint64_t kSmemMaxBytes = 192ull << 10;
 // 112 Gkeys/s; not allocating, 1-8 MiB: 128.7).
 constexpr uint64_t kL1NoAllocBytes = 256ull << 10;
 
-// Blocked Bloom filters just beyond the single-pass limit (160-240 MiB; zoned
-// ones, reading 2-4 words per key, up to 320 MiB): the bitmask plan in its
-// block-range passes with the 32-register variant beats the partitioned plan.
-// B200, 2^27 probes, Gkeys/s, bitmask vs partition:
-//   u64 w=8 s=8 k=8     168 / 192 / 224 MiB: 84.9 / 82.7 / 78.2 vs 74.3 / 74.1 / 75.1
-//   u32 w=1 k=4         168 / 192 MiB: 136.2 / 119.5 vs 102.7 / 104.1 (224: even)
-//   u32 w=16 s=1 k=4    168 / 192 / 224 MiB: 97.3 / 91.5 / 84.9 vs 67.5 / 66.6 / 65.2
-//   zoned u32 w=16 z=2  192 / 256 MiB: 110.1 / 89.7 vs 74.4 / 75.3
-//   zoned u64 w=8 z=4   192 / 256 MiB: 75.3 / 74.5 vs 67.3 / 68.7
-// but not for 32-byte blocks (u64 w=4 s=4 k=8, 168 MiB: 83.9 vs 89.7), nor
-// from 384 MiB on (zoned u64 w=8 z=2: 68.1 vs 73.7).
+// Blocked Bloom filters just beyond the single-pass limit whose words the
+// hash picks one by one (s < w), or of one word per block, and zoned u32
+// filters of 192 MiB: the bitmask plan in its block-range passes with the
+// 32-register variant beats the partitioned plan.  B200, 2^27 probes, Gkeys/s,
+// bitmask vs partition:
+//   u32 w=16 s=1 k=4    192 / 224 / 256 MiB: 106.1 / 98.1 / 90.4 vs 81.9 / 82.9 / 83.3
+//   u64 w=8 s=2 k=8     192 MiB: 75.9 vs 64.0
+//   u32 w=1 k=4         168 / 192 MiB: 136.2 / 119.5 vs 102.7 / 104.1 (256: 93.6 vs 105.9)
+//   zoned u32 w=16 z=2  192 / 256 MiB: 105.0 / 89.6 vs 97.9 / 100.6
+// Layouts that test half a block before loading the rest (s >= w with blocks
+// of >= 64 bytes) and zoned u64 ones probe faster partitioned from 160 MiB on
+// (u64 w=8 s=8 k=8 168 / 192 MiB: 89.8 / 85.5 vs 91.2 / 88.9; zoned u64 w=8
+// z=4 192 MiB: 74.6 vs 83.9; z=2 256 MiB: 87.8 vs 94.4), as do 32-byte blocks
+// (u64 w=4 s=4 k=8, 168 MiB: 83.9 vs 89.7).
 bool bitmask_band(const dtlg_filter* f) {
   if (f->d.kind != Kind::kBloom && f->d.kind != Kind::kZoned) return false;
   const uint64_t fbytes = (f->d.m_actual + 7) / 8;
   const uint64_t block_bytes = static_cast<uint64_t>(f->d.w) * f->d.word_bytes;
   if (fbytes <= (160ull << 20)) return false;
-  if (f->d.kind == Kind::kZoned) return fbytes <= (320ull << 20);
-  return fbytes <= (240ull << 20) && block_bytes != 32;  // 224 MiB requests round up under MAGIC
+  // the limits leave room for MAGIC sizes, which round a request up
+  if (f->d.kind == Kind::kZoned) return f->d.word_bytes == 4 && fbytes <= (224ull << 20);
+  if (f->d.s < f->d.w) return fbytes <= (264ull << 20);
+  return block_bytes < 32 && fbytes <= (240ull << 20);
 }
 
 int probe_plan(const dtlg_filter* f, uint64_t n) {
@@ -244,10 +249,14 @@ int probe_plan(const dtlg_filter* f, uint64_t n) {
   return mode;
 }
 
-// Register-budget variant of the bitmask / pair kernels: the caller's, else 0
-// in the band above, else 1.
-int probe_variant(const dtlg_filter* f) {
+// Register-budget variant of the bitmask / pair kernels for plan `mode`: the
+// caller's, else 0 for the bitmask plan in the band above and for the pair
+// probe of Bloom filters (u64 w=8 s=8 k=8, 192 / 256 / 512 MiB: 88.9 / 91.5 /
+// 84.9 Gkeys/s against 84.8 / 85.3 / 80.4; zoned u64 w=8 z=2 256 / 384 MiB:
+// 94.4 / 91.1 against 92.7 / 88.3; no layout measured slower), else 1.
+int probe_variant(const dtlg_filter* f, int mode) {
   if (f->bits_variant >= 0 && f->bits_variant < kBitsVariants) return f->bits_variant;
+  if (mode == 3) return (f->d.kind == Kind::kBloom || f->d.kind == Kind::kZoned) ? 0 : 1;
   return bitmask_band(f) ? 0 : 1;
 }
 
@@ -354,7 +363,7 @@ dtlg_status launch_probe(const dtlg_filter* f, const uint64_t* words, const uint
     return DTLG_OK;
   }
   uint32_t* bits = reinterpret_cast<uint32_t*>(wsb + lay.bits_off);
-  const int v = probe_variant(f);
+  const int v = probe_variant(f, mode);
   a.vec32 = (reinterpret_cast<uintptr_t>(words) & 31u) == 0 ? 1u : 0u;
   if (mode == 4) {
     // the whole filter in every CTA's shared memory

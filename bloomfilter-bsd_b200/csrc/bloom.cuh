@@ -167,8 +167,9 @@ struct BloomOps {
     return static_cast<const Word*>(filter) + static_cast<uint64_t>(blk) * kW;
   }
 
-  // Every bit of the key set?  ((word & mask) == mask over all touched words,
-  // without early out, as blocked_bloomfilter.hpp:34 configures.)
+  // Every bit of the key set?  ((word & mask) == mask over all touched words.
+  // The reference configures no early out, blocked_bloomfilter.hpp:34; the
+  // result of the conjunction is the same with one, see kHalves.)
   __device__ __forceinline__ static bool contains(const ProbeArgs& a, uint32_t key) {
     const uint32_t blk = block_index(key * mul_const(0), a.addr);
     if (a.range_on && (blk < a.blk_lo || blk >= a.blk_hi)) return false;  // another pass's block
@@ -176,21 +177,28 @@ struct BloomOps {
                             a.vec32 != 0, a.l1na != 0);
   }
 
-  // The key's bits in the block at `base`; NC selects the read-only load path.
-  template <bool NC>
-  __device__ __forceinline__ static bool test_block(const Word* base, uint32_t key, bool vec32, bool l1na = false) {
+  // The groups whose word lies in [Lo, Hi), against words v[0..Hi-Lo).
+  template <int Lo, int Hi>
+  __device__ __forceinline__ static bool test_words(const Word* v, uint32_t key) {
     bool ok = true;
-    if constexpr (kS.fixed_words) {
-      Word v[kW];
-      load_block<Word, kW, NC>(base, v, vec32, l1na);
-      static_for<kS.ng>([&](auto G) {
-        constexpr int g = decltype(G)::value;
+    static_for<kS.ng>([&](auto G) {
+      constexpr int g = decltype(G)::value;
+      constexpr int wi = kS.g[g].wconst;
+      if constexpr (wi >= Lo && wi < Hi) {
         const Word m = group_mask<g>(key);
-        ok &= (v[kS.g[g].wconst] & m) == m;
-      });
-    } else {
-      static_for<kS.ng>([&](auto G) {
-        constexpr int g = decltype(G)::value;
+        ok &= (v[wi - Lo] & m) == m;
+      }
+    });
+    return ok;
+  }
+
+  // Groups [Lo, Hi) of a layout whose words the hash picks: one word load each.
+  template <int Lo, int Hi, bool NC = true>
+  __device__ __forceinline__ static bool test_groups(const Word* base, uint32_t key) {
+    bool ok = true;
+    static_for<kS.ng>([&](auto G) {
+      constexpr int g = decltype(G)::value;
+      if constexpr (g >= Lo && g < Hi) {
         const Word m = group_mask<g>(key);
         const Word* p = base + group_word<g>(key);
         Word x;
@@ -200,7 +208,47 @@ struct BloomOps {
           x = NC ? __ldg(reinterpret_cast<const unsigned int*>(p)) : ld_weak_32(p);
         }
         ok &= (x & m) == m;
+      }
+    });
+    return ok;
+  }
+
+  // Blocks of >= 64 bytes read through the read-only path test their first
+  // half before loading the second: the match result is the same (the test is
+  // a conjunction), but most non-members fail on the first half, so the
+  // second 32-byte load is skipped for them.
+  static constexpr bool kHalves = kS.fixed_words && kW * static_cast<int>(sizeof(Word)) >= 64;
+
+  // The key's bits in the block at `base`; NC selects the read-only load path.
+  template <bool NC>
+  __device__ __forceinline__ static bool test_block(const Word* base, uint32_t key, bool vec32, bool l1na = false) {
+    if constexpr (NC && kHalves) {
+      if (vec32) {
+        constexpr int kH = kW / 2;
+        Word v[kH];
+        load_block<Word, kH>(base, v, true, l1na);
+        if (!test_words<0, kH>(v, key)) return false;
+        load_block<Word, kH>(base + kH, v, true, l1na);
+        return test_words<kH, kW>(v, key);
+      }
+    }
+    bool ok = true;
+    if constexpr (kS.fixed_words) {
+      Word v[kW];
+      load_block<Word, kW, NC>(base, v, vec32, l1na);
+      static_for<kS.ng>([&](auto G) {
+        constexpr int g = decltype(G)::value;
+        const Word m = group_mask<g>(key);
+        ok &= (v[kS.g[g].wconst] & m) == m;
       });
+    } else if constexpr (NC && kS.ng >= 2) {
+      // words picked by the hash (zoned, s < w): the first half of the groups,
+      // then, for the keys that pass, the second half
+      constexpr int kG = kS.ng / 2;
+      if (!test_groups<0, kG>(base, key)) return false;
+      return test_groups<kG, kS.ng>(base, key);
+    } else {
+      ok = test_groups<0, kS.ng, NC>(base, key);
     }
     return ok;
   }
