@@ -213,22 +213,30 @@ struct BloomOps {
     return ok;
   }
 
-  // Blocks of >= 64 bytes read through the read-only path test their first
-  // half before loading the second: the match result is the same (the test is
-  // a conjunction), but most non-members fail on the first half, so the
-  // second 32-byte load is skipped for them.
+  // Blocks of >= 64 bytes test their first half before loading the second:
+  // the match result is the same (the test is a conjunction), but most
+  // non-members fail on the first half, so the second 32-byte load is skipped
+  // for them.
   static constexpr bool kHalves = kS.fixed_words && kW * static_cast<int>(sizeof(Word)) >= 64;
 
   // The key's bits in the block at `base`; NC selects the read-only load path.
   template <bool NC>
   __device__ __forceinline__ static bool test_block(const Word* base, uint32_t key, bool vec32, bool l1na = false) {
-    if constexpr (NC && kHalves) {
-      if (vec32) {
-        constexpr int kH = kW / 2;
+    if constexpr (kHalves) {
+      constexpr int kH = kW / 2;
+      if constexpr (NC) {
+        if (vec32) {
+          Word v[kH];
+          load_block<Word, kH>(base, v, true, l1na);
+          if (!test_words<0, kH>(v, key)) return false;
+          load_block<Word, kH>(base + kH, v, true, l1na);
+          return test_words<kH, kW>(v, key);
+        }
+      } else {
         Word v[kH];
-        load_block<Word, kH>(base, v, true, l1na);
+        load_block<Word, kH, false>(base, v);
         if (!test_words<0, kH>(v, key)) return false;
-        load_block<Word, kH>(base + kH, v, true, l1na);
+        load_block<Word, kH, false>(base + kH, v);
         return test_words<kH, kW>(v, key);
       }
     }
@@ -241,12 +249,12 @@ struct BloomOps {
         const Word m = group_mask<g>(key);
         ok &= (v[kS.g[g].wconst] & m) == m;
       });
-    } else if constexpr (NC && kS.ng >= 2) {
+    } else if constexpr (kS.ng >= 2) {
       // words picked by the hash (zoned, s < w): the first half of the groups,
       // then, for the keys that pass, the second half
       constexpr int kG = kS.ng / 2;
-      if (!test_groups<0, kG>(base, key)) return false;
-      return test_groups<kG, kS.ng>(base, key);
+      if (!test_groups<0, kG, NC>(base, key)) return false;
+      return test_groups<kG, kS.ng, NC>(base, key);
     } else {
       ok = test_groups<0, kS.ng, NC>(base, key);
     }
