@@ -251,9 +251,11 @@ int probe_plan(const dtlg_filter* f, uint64_t n) {
 
 // Register-budget variant of the bitmask / pair kernels for plan `mode`: the
 // caller's, else 0 for the bitmask plan in the band above and for the pair
-// probe of Bloom filters (u64 w=8 s=8 k=8, 192 / 256 / 512 MiB: 88.9 / 91.5 /
-// 84.9 Gkeys/s against 84.8 / 85.3 / 80.4; zoned u64 w=8 z=2 256 / 384 MiB:
-// 94.4 / 91.1 against 92.7 / 88.3; no layout measured slower), else 1.
+// probe of Bloom filters, else 1.  Pair probe, v0 against v1, Gkeys/s:
+// u64 w=8 s=8 k=8 at 192 / 256 / 512 MiB 88.9 / 91.5 / 84.9 against 84.8 /
+// 85.3 / 80.4 with 32 MiB ranges, 92.2 / 94.3 / 89.0 against 89.7 / 92.1 /
+// 90.5 with 8 MiB ranges; zoned u64 w=8 z=2 at 256 / 384 MiB 94.4 / 91.1
+// against 92.7 / 88.3.
 int probe_variant(const dtlg_filter* f, int mode) {
   if (f->bits_variant >= 0 && f->bits_variant < kBitsVariants) return f->bits_variant;
   if (mode == 3) return (f->d.kind == Kind::kBloom || f->d.kind == Kind::kZoned) ? 0 : 1;
