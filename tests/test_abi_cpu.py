@@ -107,3 +107,28 @@ def test_default_configs_match_reference():
     assert (c.k, c.word_size, c.word_cnt_per_block, c.sector_cnt, c.addr_mode, c.zone_cnt) == (8, 4, 1, 1, 0, 1)
     d = F.cuckoofilter_config()
     assert (d.bits_per_tag, d.tags_per_bucket, d.addr_mode) == (8, 2, 0)
+
+
+@pytest.mark.parametrize("cfg,mib,plan", [
+    # (word bytes, words, sectors, zones, k), filter MiB, expected automatic plan
+    ((8, 8, 8, 1, 8), 128, 2), ((8, 8, 8, 1, 8), 168, 3), ((8, 8, 8, 1, 8), 512, 3),
+    ((8, 4, 4, 1, 8), 192, 3),                       # 32-byte blocks: partitioned
+    ((4, 1, 1, 1, 4), 168, 2), ((4, 1, 1, 1, 4), 256, 3),
+    ((4, 16, 1, 1, 4), 224, 2), ((4, 16, 1, 1, 4), 256, 2), ((4, 16, 1, 1, 4), 384, 3),
+    ((8, 8, 2, 1, 8), 192, 2),
+    ((4, 16, 16, 2, 8), 192, 2), ((4, 16, 16, 2, 8), 256, 3),
+    ((8, 8, 8, 2, 8), 256, 3), ((8, 8, 8, 4, 8), 192, 3),
+])
+def test_automatic_probe_plan(cfg, mib, plan):
+    """The planner's choice for 2^28 probes (host logic only): the bitmask plan
+    in block-range passes up to 160 MiB and, beyond, in the band of layouts it
+    was measured faster for (s < w, one-word blocks, zoned u32); the
+    partitioned plan (5 kernels) otherwise.  Fewer than 2^20 keys: the fused
+    single-kernel plan."""
+    wb, w, s, z, k = cfg
+    f = F.construct(F.blocked_bloomfilter_config(k=k, word_size=wb, word_cnt_per_block=w, sector_cnt=s,
+                                                 zone_cnt=z), mib << 23)
+    L = _lib.lib()
+    kernels = L.dtlg_probe_kernel_count(f._h, 1 << 28)
+    assert (kernels == 5) == (plan == 3), (cfg, mib, kernels)
+    assert L.dtlg_probe_kernel_count(f._h, (1 << 20) - 1) == 1
