@@ -167,18 +167,78 @@ def workload_config(name, n_gpus):
 
 # ---------------------------------------------------------------------------
 class ClockSampler:
-    """nvidia-smi clocks / throttle reasons sampled during the timed region."""
+    """SM clocks and throttle reasons during the timed region.  NVML is polled
+    every 2 ms in a thread and the samples between mark_start() and mark_end()
+    are kept (a 20-step timed region lasts only tens of ms).  Without NVML,
+    nvidia-smi -lms 100 samples from start() to stop() instead.  Reads only."""
 
     Q = ("index,clocks.sm,clocks.max.sm,power.draw,clocks_event_reasons.active,"
          "clocks_event_reasons.hw_slowdown,clocks_event_reasons.hw_thermal_slowdown,"
          "clocks_event_reasons.sw_thermal_slowdown,clocks_event_reasons.sw_power_cap")
+    NAMES = ("hw_slowdown", "hw_thermal_slowdown", "sw_thermal_slowdown", "sw_power_cap")
+    # NVML clocks-event reason bits of the same four (nvml.h)
+    NVML_BITS = {"hw_slowdown": 0x8, "hw_thermal_slowdown": 0x40, "sw_thermal_slowdown": 0x20, "sw_power_cap": 0x4}
 
-    def __init__(self, gpu_index):
+    def __init__(self, gpu_index, nvml=None):
         self.gpu = gpu_index
         self.proc = None
         self.path = None
+        self.nvml = nvml            # the NVML module (pynvml unless given)
+        self._nv = None
+        self.thread = None
+        self.samples = []           # (perf_counter, sm MHz, reason bits)
+        self.t0 = self.t1 = None
+        self.max_mhz = None
+        self.stop_evt = threading.Event()
 
     def start(self):
+        if not self._start_nvml():
+            self._start_smi()
+
+    def mark_start(self):
+        self.t0 = time.perf_counter()
+
+    def mark_end(self):
+        self.t1 = time.perf_counter()
+
+    def _start_nvml(self):
+        try:
+            nv = self.nvml
+            if nv is None:
+                import pynvml as nv
+            nv.nvmlInit()
+            try:
+                import torch
+                p = torch.cuda.get_device_properties(self.gpu)
+                h = nv.nvmlDeviceGetHandleByPciBusId(
+                    f"{p.pci_domain_id:08x}:{p.pci_bus_id:02x}:{p.pci_device_id:02x}.0")
+            except Exception:
+                h = nv.nvmlDeviceGetHandleByIndex(self.gpu)
+            self.max_mhz = float(nv.nvmlDeviceGetMaxClockInfo(h, nv.NVML_CLOCK_SM))
+            self._reasons = (getattr(nv, "nvmlDeviceGetCurrentClocksEventReasons", None)
+                             or nv.nvmlDeviceGetCurrentClocksThrottleReasons)
+            self._nv, self._h = nv, h
+            self._poll()            # a failing query fails here, not in the thread
+            self.thread = threading.Thread(target=self._run, daemon=True)
+            self.thread.start()
+            return True
+        except Exception:
+            self._nv = None
+            return False
+
+    def _poll(self):
+        t = time.perf_counter()
+        sm = float(self._nv.nvmlDeviceGetClockInfo(self._h, self._nv.NVML_CLOCK_SM))
+        self.samples.append((t, sm, int(self._reasons(self._h))))
+
+    def _run(self):
+        while not self.stop_evt.wait(0.002):
+            try:
+                self._poll()
+            except Exception:
+                return
+
+    def _start_smi(self):
         try:
             fd, self.path = tempfile.mkstemp(suffix=".csv")
             os.close(fd)
@@ -189,6 +249,23 @@ class ClockSampler:
             self.proc = None
 
     def stop(self):
+        if self.thread is not None:
+            self.stop_evt.set()
+            self.thread.join(timeout=2)
+            try:
+                self._nv.nvmlShutdown()
+            except Exception:
+                pass
+            done = list(self.samples)
+            win = [x for x in done if self.t0 is not None and self.t1 is not None and self.t0 <= x[0] <= self.t1]
+            used = win or done
+            reasons = {nm for nm, bit in self.NVML_BITS.items() for _, _, r in used if r & bit}
+            return {"sm_mhz": statistics.median(x[1] for x in used), "sm_max_mhz": self.max_mhz,
+                    "reasons": sorted(reasons), "samples": len(used),
+                    "source": "NVML every 2 ms, " + ("timed region" if win else "whole run")}
+        return self._stop_smi()
+
+    def _stop_smi(self):
         if not self.proc:
             return None
         self.proc.terminate()
@@ -197,7 +274,6 @@ class ClockSampler:
         except Exception:
             self.proc.kill()
         sm, mx, reasons = [], None, set()
-        names = ["hw_slowdown", "hw_thermal_slowdown", "sw_thermal_slowdown", "sw_power_cap"]
         for line in open(self.path):
             p = [x.strip() for x in line.split(",")]
             if len(p) < 9:
@@ -207,14 +283,14 @@ class ClockSampler:
                 mx = float(p[2])
             except ValueError:
                 continue
-            for nm, v in zip(names, p[5:9]):
+            for nm, v in zip(self.NAMES, p[5:9]):
                 if v.lower() == "active":
                     reasons.add(nm)
         os.unlink(self.path)
         if not sm:
             return None
         return {"sm_mhz": statistics.median(sm), "sm_max_mhz": mx, "reasons": sorted(reasons),
-                "samples": len(sm)}
+                "samples": len(sm), "source": "nvidia-smi every 100 ms, whole run"}
 
 
 def load_traffic_profile():
@@ -403,6 +479,7 @@ def run_dtlg(args):
     evs = [(torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)) for _ in range(args.steps)]
     t_start = torch.cuda.Event(enable_timing=True)
     t_end = torch.cuda.Event(enable_timing=True)
+    clocks.mark_start()
     t_start.record(stream)
     for i in range(args.steps):
         evs[i][0].record(stream)
@@ -410,6 +487,7 @@ def run_dtlg(args):
         evs[i][1].record(stream)
     t_end.record(stream)
     torch.cuda.synchronize()
+    clocks.mark_end()
     if world > 1:
         dist.barrier()
     clk = clocks.stop()
@@ -783,8 +861,10 @@ def run_batched(args):
     steps = max(3, min(args.steps, 20))
     clocks = ClockSampler(int(os.environ.get("LOCAL_RANK", "0")))
     clocks.start()
+    clocks.mark_start()
     ms_batched = timed(batched_step, steps)
     ms_per_filter = timed(per_filter_step, steps)
+    clocks.mark_end()
     clk = clocks.stop()
     per_filter_kernels = sum((1 if it.build_keys.numel() else 0) + L.dtlg_probe_kernel_count(it.filter._h,
                                                                                            it.probe_keys.numel())
