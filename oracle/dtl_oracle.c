@@ -1,7 +1,7 @@
 /*
  * dtl_oracle.c -- CPU restatement of the DTL filter build/probe path.
  *
- * TEST INFRASTRUCTURE ONLY (the checker, never the product): see dtl_oracle.h.
+ * TEST INFRASTRUCTURE ONLY (the oracle the tests compare against, never the product): see dtl_oracle.h.
  *
  * Every function below restates the behaviour of the reference
  * (peterboncz/bloomfilter-bsd, paths relative to that project) in plain C.

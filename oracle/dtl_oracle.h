@@ -1,7 +1,7 @@
 /*
  * dtl_oracle.h -- CPU restatement of the DTL filter build/probe path.
  *
- * TEST INFRASTRUCTURE ONLY.  This library is the checker for the CUDA path:
+ * TEST INFRASTRUCTURE ONLY.  This library is the oracle for the CUDA path:
  * only tests/, __graft_entry__.smoke() and bench.py's cpu_baseline leg may load
  * it.  The product library (libdtlg.so) never links or calls it.
  *

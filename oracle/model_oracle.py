@@ -1,6 +1,6 @@
 """Oracle of the configuration-choice path (TEST INFRASTRUCTURE ONLY).
 
-Used by tests/ as the checker; the product never imports it.
+Used by tests/ as the oracle; the product never imports it.
 
   * FPR formulas as plain Python loops, step for step as the reference writes
     them (src/dtl/filter/blocked_bloomfilter/fpr.hpp:12-61, math.hpp:17-205),
