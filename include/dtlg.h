@@ -171,19 +171,23 @@ dtlg_status dtlg_batch_contains_gather(const dtlg_filter* f, const uint64_t* fil
 /* Probe tuning of one filter (set by the autotuner, dtlg_autotune_probe):
  * mode 0 = automatic, 1 = one fused kernel (probe + ordered compaction),
  * 2 = two streaming kernels (match bitmask, then compaction), 3 = partitioned
- * (keys sorted into L2-sized block ranges; Bloom and blocked cuckoo filters),
+ * (keys sorted into ~8 MiB block ranges; Bloom and blocked cuckoo filters),
  * 4 = match bitmask against a copy of the filter in every CTA's shared memory
  * (Bloom and classic Bloom filters of at most 192 KiB); a plan the filter does
- * not offer falls back to 2.  variant selects
- * the register budget of the bitmask kernel (-1 = automatic, 0 = 32 registers
- * at 8 CTAs/SM, 1 = 64 registers at 4 CTAs/SM).  Results never change.
+ * not offer falls back to 2.  Automatic: 1 below 2^20 keys; 3 for filters
+ * beyond 160 MiB, except Bloom layouts measured faster in plan 2 (words picked
+ * by the hash, s < w, up to 256 MiB; blocks under 32 bytes up to 240 MiB;
+ * zoned u32 up to 224 MiB); else 2.  variant selects the register budget of
+ * the bitmask and pair kernels (-1 = automatic: 0 for the pair probe of Bloom
+ * filters and for plan 2 in the exceptions above, else 1; 0 = 32 registers at
+ * 8 CTAs/SM, 1 = 64 registers at 4 CTAs/SM).  Results never change.
  * (The reference's counterpart is its per-config SIMD unroll factor,
  * blocked_bloomfilter_tune.hpp:21-56.) */
 dtlg_status dtlg_set_probe_options(dtlg_filter* f, int mode, int variant);
 /* Build plan of a blocked Bloom or blocked cuckoo filter (no counterpart in
  * the reference, whose batch_insert is one loop): 0 = automatic (2 for Bloom
  * filters beyond 160 MiB and batches of >= 2^20 keys, else 1), 1 = one kernel of
- * global atomics, 2 = keys first grouped by L2-sized block range (the
+ * global atomics, 2 = keys first grouped by ~8 MiB block range (the
  * partitioned probe's partition, 8 bytes per key of workspace from the
  * library's stream-ordered pool; without room there, plan 1), then inserted
  * range by range so the atomics hit L2.  Bloom filter
