@@ -16,6 +16,15 @@
 // uses; two calls whose kernels overlap on the GPU (different streams without
 // ordering between them, or several host threads) race on it and must be
 // serialized by the caller.
+//
+// It always runs the fused single-kernel probe (plan 1): the scratch has no
+// room for the match bitmask or the key pairs of the other plans, so filters
+// far beyond L2 probe slower here than through dtlg_batch_contains_async, with
+// the same results.  A look-back wait that gives up leaves UINT64_MAX in
+// *match_cnt_dev (the error word itself stays in the shared scratch).  The
+// array's device address is resolved once per device and kept for the life of
+// the process; after a cudaDeviceReset it would be stale, so the entry point
+// is not for processes that reset their devices.
 #include <cuda_runtime.h>
 
 #include <algorithm>

@@ -143,7 +143,12 @@ dtlg_status dtlg_batch_insert(const dtlg_filter* f, uint64_t* filter_words, cons
 dtlg_status dtlg_batch_contains(const dtlg_filter* f, const uint64_t* filter_words,
                                 const uint32_t* keys, uint32_t key_cnt, uint32_t* match_positions,
                                 uint32_t match_offset, uint64_t* match_cnt, dtlg_stream_t stream);
-/* Fully asynchronous form: the count goes to *match_cnt_dev (DEVICE pointer). */
+/* Fully asynchronous form: the count goes to *match_cnt_dev (DEVICE pointer).
+ * The asynchronous forms (_async, _ws, _gather, _noalloc) cannot return
+ * DTLG_ERR_TIMEOUT, since the status is known only on the device: when one of
+ * the probe's bounded device waits gives up, *match_cnt_dev is set to
+ * UINT64_MAX and the positions are invalid.  Read the count as
+ * DTLG_ERR_TIMEOUT in that case (dtlg_batch_contains does so itself). */
 dtlg_status dtlg_batch_contains_async(const dtlg_filter* f, const uint64_t* filter_words,
                                       const uint32_t* keys, uint32_t key_cnt,
                                       uint32_t* match_positions, uint32_t match_offset,
@@ -237,8 +242,15 @@ dtlg_status dtlg_autotune_probe(dtlg_filter* f, const uint64_t* filter_words, co
  * array of about 128 KiB per GPU, held until exit; key_cnt above
  * DTLG_NOALLOC_MAX_KEYS is rejected with DTLG_ERR_WORKSPACE.  The first call
  * on each device looks the array's address up (make that first call before
- * any stream capture).  All calls share the array: calls that overlap on the
- * GPU race and must be serialized by the caller. */
+ * any stream capture); the address is kept for the life of the process, so
+ * the entry point must not be used after a cudaDeviceReset of that device.
+ * All calls share the array: calls that overlap on the GPU race and must be
+ * serialized by the caller.  It always runs the single fused probe kernel
+ * (its scratch has no room for a match bitmask or key pairs) and ignores the
+ * plan of dtlg_set_probe_options / dtlg_autotune_probe: the results are the
+ * same, but filters far beyond L2 probe about 2-2.5x slower than with the
+ * bitmask or partitioned plans that dtlg_batch_contains_async picks there.
+ * A bounded device wait that gives up leaves UINT64_MAX in *match_cnt_dev. */
 #define DTLG_NOALLOC_MAX_KEYS (1u << 26)
 dtlg_status dtlg_batch_contains_noalloc(const dtlg_filter* f, const uint64_t* filter_words,
                                         const uint32_t* keys, uint32_t key_cnt,

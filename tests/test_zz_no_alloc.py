@@ -5,8 +5,9 @@ buffer manager or host application, or an allocation's synchronization is too
 costly on their path).  This entry point keeps the probe's scratch in a static
 device array instead; its results must equal the ordinary entry point's.
 Checked through the C ABI on two calls in a row (the shared array keeps the
-previous call's contents, so the second call shows that it is cleared), for a
-Bloom and a cuckoo filter, plus the rejection of oversized calls.
+previous call's contents, so the second call shows that it is cleared), for
+every filter kind (blocked Bloom, zoned Bloom, cuckoo, blocked cuckoo, classic
+Bloom), plus the rejection of oversized calls.
 
 Named test_zz_* so that pytest collects it last.
 """
@@ -85,6 +86,26 @@ def test_noalloc_cuckoo_matches_existing_entry_point_twice():
     for seed, n in ((43, 300_000), (44, 7)):
         keys = dev(keygen.probe_keys(60000, n, 0.4, seed)[0])
         assert np.array_equal(probe_noalloc(f, words, keys, 0), probe_existing(f, words, keys, 0))
+
+
+@pytest.mark.parametrize("kind", ["zoned", "blocked_cuckoo", "classic"])
+def test_noalloc_other_kinds_match_existing_entry_point_twice(kind):
+    """The zoned, blocked cuckoo and classic kinds reach the same fused kernel
+    with their own filter arguments; each is built on the GPU and probed twice
+    in a row (a large call, then a small one from a misaligned key pointer)."""
+    n = 80000
+    if kind == "zoned":
+        f = dtlg.zbbf_64(12 * n + 5, 8, 8, 4)
+    elif kind == "blocked_cuckoo":
+        f = dtlg.bcf(1 << 21, 64, 16, 4)
+    else:
+        f = dtlg.bloomfilter_logic(16 * n, 5, dtlg.MAGIC)
+    words = f.alloc_filter_data()
+    assert f.batch_insert(words, dev(keygen.build_keys(n, 45)))
+    k1 = dev(keygen.probe_keys(n, 700_001, 0.25, 45)[0])
+    k2 = dev(keygen.probe_keys(n, 33_333, 0.5, 46)[0])[3:]
+    for keys, off in ((k1, 11), (k2, 0)):
+        assert np.array_equal(probe_noalloc(f, words, keys, off), probe_existing(f, words, keys, off))
 
 
 def test_noalloc_rejects_more_keys_than_its_scratch_serves():
