@@ -76,6 +76,8 @@ def parse():
     ap.add_argument("--batch-filters", type=int, default=512, help="batched512: number of filters")
     ap.add_argument("--batch-max-log2", type=int, default=24, help="batched512: log2 of the largest n / probes")
     ap.add_argument("--no-e2e", action="store_true")
+    ap.add_argument("--no-batched", action="store_true",
+                    help="sectorized_dram: skip the batched-vs-per-filter comparison the default line carries")
     ap.add_argument("--probe-mode", type=int, default=0,
                     help="0 auto, 1 fused, 2 bitmask + block-range passes, 3 partitioned, 4 shared-memory filter copy")
     ap.add_argument("--probe-passes", type=int, default=0, help="block-range passes of mode 2 (0 auto)")
@@ -314,61 +316,90 @@ def load_peaks():
 
 
 # ---------------------------------------------------------------------------
-def cpu_reference_probe(words_np, cfg, m, probe_np, threads, budget_s, want_kind="reference"):
-    """The reference's own SIMD batch_contains (oracle/_ref) -- or, if that
-    library is absent, the C restatement -- on a bounded sample of the probe
-    stream, all host threads.  Returns (keys/s, kind, sample keys, count)."""
-    sys.path.insert(0, os.path.join(ROOT, "oracle"))
-    import numpy as np
+# The reference's CPU path, one method for both arms: the reference's own
+# batch_contains (oracle/_ref: its filter logic compiled from its sources) on
+# all host threads, each thread on its own contiguous slice in 1024-key batches
+# (model/benchmark.cpp:123-165, batchwise.hpp:9), with the SIMD unroll factor
+# the reference's own calibration picks (blocked_bloomfilter_tune_impl.hpp:
+# 162-256, cuckoofilter_tune_impl.hpp:118-225).  The sample is the first
+# REF_SAMPLE keys of the workload's probe stream; the statistic is keys over
+# the summed time of the timed runs (the mean rate).
+REF_SAMPLE = 1 << 26
 
-    import oracle as O
-    out = np.empty(len(probe_np) + 64, dtype=np.uint32)
-    if cfg[0] == "classic":
-        ref = O.try_refcbf() if want_kind == "reference" else None
-        if ref is None:
-            raise RuntimeError("the reference's bloomfilter_logic is not built (oracle/_ref)")
-        f = ref.create(cfg[1], m, cfg[2])
-        words_u32 = np.zeros(f.size_u32 + 16, dtype=np.uint32)
-        words_u32[: f.size_u32] = words_np.view(np.uint32)[: f.size_u32]
-        kind = "reference"
-        run = lambda keys: f.batch_contains_mt(words_u32, keys, threads, out=out)  # noqa: E731
-    elif cfg[0] == "bcf":
-        ref = bcf_reference() if want_kind == "reference" else None
-        if ref is None:
-            raise RuntimeError("the reference's dtl::bcf is not built (oracle/_ref)")
-        f = ref.create(m, cfg[1], cfg[2], cfg[3])
-        words_u32 = np.zeros(f.size_u32 + 16, dtype=np.uint32)
-        words_u32[: f.size_u32] = words_np.view(np.uint32)[: f.size_u32]
-        kind = "reference"
-        run = lambda keys: f.batch_contains_mt(words_u32, keys, threads, out=out)  # noqa: E731
-    else:
-        ref = O.try_reflib() if want_kind == "reference" else None
-        f = None
-        if ref is not None:
-            f = ref.cuckoo(cfg[1], cfg[2], m) if cfg[0] == "cuckoo" else ref.bloom(*cfg, m)
-        if f is not None:
-            kind = "reference"
-            run = lambda keys: f.batch_contains_mt(words_np, keys, threads, unroll=1, out=out)  # noqa: E731
+
+class RefProbe:
+    """The reference's probe of one workload's filter on the host."""
+
+    def __init__(self, cfg, m, words_np, threads):
+        sys.path.insert(0, os.path.join(ROOT, "oracle"))
+        import numpy as np
+
+        import oracle as O
+        self.threads = threads
+        self.unroll, self.unroll_ns = None, None
+        if cfg[0] in ("classic", "bcf"):
+            ref = O.try_refcbf() if cfg[0] == "classic" else bcf_reference()
+            if ref is None:
+                raise RuntimeError(f"the reference's {cfg[0]} filter is not built (oracle/_ref)")
+            f = ref.create(cfg[1], m, cfg[2]) if cfg[0] == "classic" else ref.create(m, cfg[1], cfg[2], cfg[3])
+            words = np.zeros(f.size_u32 + 16, dtype=np.uint32)
+            words[: f.size_u32] = words_np.view(np.uint32)[: f.size_u32]
+            self.variant = "scalar" if cfg[0] == "classic" else ref.variant
+            # neither has an unroll parameter (bcf.cpp, bloomfilter_logic.hpp)
+            self._count = lambda keys, out: f.batch_contains_mt(words, keys, threads, out=out)  # noqa: E731
+            self._list = lambda keys, out: f.batch_contains_mt_list(words, keys, threads, out=out)  # noqa: E731
         else:
-            if cfg[0] == "cuckoo":
-                raise RuntimeError("the reference build lacks this cuckoo config")
-            f = O.Bloom(*cfg, m)
-            kind = "port"
-            run = lambda keys: f.batch_contains_mt(words_np, keys, threads)  # noqa: E731
-    # size the sample so one pass takes about budget_s
-    n = min(len(probe_np), 1 << 20)
-    t0 = time.perf_counter()
-    run(probe_np[:n])
-    dt = max(time.perf_counter() - t0, 1e-6)
-    n = int(min(len(probe_np), max(n, n * budget_s / dt)))
-    best = None
-    cnt = 0
-    for _ in range(2):
-        t0 = time.perf_counter()
-        cnt = run(probe_np[:n])
-        dt = time.perf_counter() - t0
-        best = dt if best is None else min(best, dt)
-    return n / best, kind, n, cnt, (ref.variant if kind == "reference" else "c")
+            ref = O.try_reflib()
+            if ref is None:
+                raise RuntimeError("the reference's filter logic is not built (oracle/_ref)")
+            f = ref.cuckoo(cfg[1], cfg[2], m) if cfg[0] == "cuckoo" else ref.bloom(*cfg, m)
+            if f is None:
+                raise RuntimeError("this configuration is not instantiated in oracle/_ref")
+            words = words_np
+            self.variant = f"{ref.variant}, {ref.lanes} lanes"
+            self.unroll, per = f.calibrate_unroll(words, cuckoo=cfg[0] == "cuckoo")
+            self.unroll_ns = {str(u): round(v, 3) for u, v in per.items()}
+            u = self.unroll
+            self._count = lambda keys, out: f.batch_contains_mt(words, keys, threads, unroll=u, out=out)  # noqa: E731
+            self._list = lambda keys, out: f.batch_contains_mt_list(words, keys, threads, unroll=u, out=out)  # noqa: E731
+
+    def rate(self, probe_np, runs, warmup=1):
+        """(keys/s, sample keys, count, seconds per run) over the sample."""
+        import numpy as np
+        n = min(len(probe_np), REF_SAMPLE)
+        out = np.empty(n + 64, dtype=np.uint32)
+        keys = probe_np[:n]
+        for _ in range(max(1, warmup)):
+            self._count(keys, out)
+        total, cnt = 0.0, 0
+        for _ in range(max(1, runs)):
+            t0 = time.perf_counter()
+            cnt = self._count(keys, out)
+            total += time.perf_counter() - t0
+        return n * runs / total, n, int(cnt), total / runs
+
+    def positions(self, probe_np):
+        """The reference's whole ascending match list of these keys."""
+        import numpy as np
+        out = np.empty(len(probe_np) + 64, dtype=np.uint32)
+        return self._list(probe_np, out)
+
+    def describe(self):
+        u = "" if self.unroll is None else f", unroll u={self.unroll} (the reference's calibration)"
+        return (f"{self.threads} threads x 1024-key batches (model/benchmark.cpp:123-165), "
+                f"the reference's batch_contains ({self.variant}{u})")
+
+
+def list_checksum(pos):
+    """Order-sensitive checksum of a position list: sum of pos[i] * (2i + 1)
+    mod 2^64 (any reordering, loss or change of a position changes it)."""
+    import numpy as np
+    total = np.uint64(0)
+    for b in range(0, len(pos), 1 << 24):
+        p = np.asarray(pos[b:b + (1 << 24)], dtype=np.uint64)
+        w = np.arange(2 * b + 1, 2 * (b + len(p)) + 1, 2, dtype=np.uint64)
+        total = total + (p * w).sum(dtype=np.uint64)
+    return int(total)
 
 
 def bcf_reference():
@@ -473,6 +504,9 @@ def run_dtlg(args):
     count = int(cnt_dev.item())
     # correctness of the bench's own output: every member found, positions in range
     assert count >= n_members, (count, n_members)
+    # the GPU's whole match list, checked against the reference's after timing
+    check_parity = rank == 0 and world == 1 and not args.no_cpu_baseline
+    gpu_positions = out[:count].cpu().numpy().view(np.uint32).copy() if check_parity else None
     if world > 1:
         dist.barrier()
     torch.cuda.synchronize()
@@ -538,7 +572,7 @@ def run_dtlg(args):
         keys_h = torch.empty(P, dtype=torch.int32, pin_memory=True)
         keys_h.copy_(keys)
         pos_h = torch.empty(P, dtype=torch.int32, pin_memory=True)
-        del out
+        out = None
         torch.cuda.empty_cache()
         cnt = C.c_uint64(0)
 
@@ -572,8 +606,10 @@ def run_dtlg(args):
                          "api": "dtlg_batch_contains_host (pinned host keys -> host positions)"}
         result["gpu_launches"] += e_steps * chunks * L.dtlg_probe_kernel_count(f._h, 1 << 24)
 
-    # the reference's CPU path on this host, bounded sample (rank 0, N=1 only)
-    if rank == 0 and world == 1 and not args.no_cpu_baseline:
+    # the reference's CPU path on this host (rank 0, N=1 only): its rate on a
+    # bounded sample, and its whole match list of the same 2^28 keys against
+    # the same filter words, compared with the GPU's list
+    if check_parity:
         try:
             threads = len(os.sched_getaffinity(0))
             words_np = words.cpu().numpy().view(np.uint64)
@@ -586,14 +622,43 @@ def run_dtlg(args):
                 fcfg = ("classic", ck, cmagic)
             else:
                 fcfg = (wb, w, s, z, k)
-            rate, kind, n, c, variant = cpu_reference_probe(words_np, fcfg, m, probe_np, threads, budget_s=4.0)
+            rp = RefProbe(fcfg, m, words_np, threads)
+            rate, n, c, _ = rp.rate(probe_np, runs=5)
             result["cpu_baseline"] = {"value": round(rate / 1e9, 4), "unit": "Gkeys/s", "cores": threads,
-                                      "kind": kind,
-                                      "sample": f"first {n} probe keys of this workload, best of 2, "
-                                                f"{threads} threads x 1024-key batches, {variant} build",
+                                      "kind": "reference",
+                                      "sample": f"first {n} probe keys of this workload, mean of 5 runs, "
+                                                + rp.describe(),
+                                      "unroll": rp.unroll, "unroll_ns_per_key": rp.unroll_ns,
                                       "match_count": c}
+            ref_positions = rp.positions(probe_np)
+            same = len(ref_positions) == len(gpu_positions) and bool(np.array_equal(ref_positions, gpu_positions))
+            result["parity"] = same
+            result["parity_check"] = {
+                "keys": P, "gpu_count": int(len(gpu_positions)), "reference_count": int(len(ref_positions)),
+                "gpu_checksum": list_checksum(gpu_positions), "reference_checksum": list_checksum(ref_positions),
+                "checksum": "sum of pos[i] * (2i + 1) mod 2^64 over the whole ascending list",
+                "method": "the reference's batch_contains over every probe key of this step, same filter words"}
         except Exception as e:  # the baseline is reported, never required
             result["cpu_baseline"] = {"value": None, "error": str(e)[:200]}
+            result["parity"] = None
+
+    # the metric's second half, batched vs per-filter launches (BASELINE's
+    # 512-filter configuration), on the same GPU after the probe workload
+    if world == 1 and args.workload == "sectorized_dram" and not args.no_batched:
+        words = keys = ws = out = None
+        torch.cuda.empty_cache()
+        br = batched_bench(args)
+        result["batched"] = {
+            "workload": "batched512", "filters": br["config"]["filters"],
+            "build_keys_total": br["config"]["build_keys_total"],
+            "probe_keys_total": br["config"]["probe_keys_total"],
+            "ms_batched": br["ms_per_step"], "ms_per_filter": br["per_filter"]["ms_per_step"],
+            "speedup_vs_per_filter": br["speedup_vs_per_filter"],
+            "probe_gkeys_s_batched": br["value"], "kernels_batched": br["gpu_launches"] // br["steps"],
+            "kernels_per_filter": br["per_filter"]["kernels_per_step"],
+            "bit_exact_vs_per_filter": br["bit_exact_vs_per_filter"], "steps": br["steps"],
+            "step": br["config"]["step"]}
+        result["gpu_launches"] += br["gpu_launches"]
 
     if world > 1:
         # the probe's one exchange: every rank's match count (places its
@@ -609,9 +674,12 @@ def run_dtlg(args):
 
 
 def run_reference(args):
-    """The reference's own CPU implementation of the path (oracle/_ref: its
-    blocked_bloomfilter_logic compiled from its sources), all host threads,
-    same workload / metric; rank 0 only."""
+    """The reference's own CPU implementation of the path, same workload /
+    metric, rank 0 only: the filter is built by the reference's insert
+    (oracle/_ref: its filter logic, dtl::bcf or bloomfilter_logic compiled from
+    its sources) and each step is one probe of the same sample as the GPU
+    arm's cpu_baseline (RefProbe: all host threads, the reference's calibrated
+    unroll factor)."""
     rank = int(os.environ.get("RANK", "0"))
     world = int(os.environ.get("WORLD_SIZE", "1"))
     if rank != 0:
@@ -622,136 +690,72 @@ def run_reference(args):
     from concurrent.futures import ThreadPoolExecutor
 
     from dtlg import keygen
-    ref = O.try_reflib()
-    if ref is None:
-        print(json.dumps({"impl": "reference", "unavailable": "oracle/_ref (the reference compiled from its "
-                                                               "sources) is not built on this machine"}))
-        return
     threads = len(os.sched_getaffinity(0))
     chunk = 1 << 24
+
+    def unavailable(why):
+        print(json.dumps({"impl": "reference", "unavailable": why}), flush=True)
+
     if args.workload in BCF_WORKLOADS or args.workload in CLASSIC_WORKLOADS:
-        run_reference_bcf(args, threads, chunk)
-        return
-    if args.workload in CUCKOO_WORKLOADS:
-        t, b, ln, lf, lp, hit = CUCKOO_WORKLOADS[args.workload]
-        n_build, P = 1 << ln, 1 << lp
-        m = cuckoo_bits(n_build, t, b, lf)
-        f = ref.cuckoo(t, b, m)
-        # table words plus the victim record the reference keeps after them
-        words = np.zeros((f.word_cnt * 4 + 64) // 8, dtype=np.uint64)
-    else:
-        wb, w, s, z, k, ln, bpk, lp, hit = WORKLOADS[args.workload]
-        n_build, P = 1 << ln, 1 << lp
-        m = n_build * bpk
-        f = ref.bloom(wb, w, s, z, k, m)
-        words = np.zeros((f.word_cnt * wb + 7) // 8, dtype=np.uint64)
-    if f is None:
-        print(json.dumps({"impl": "reference", "unavailable": "this configuration is not instantiated in the "
-                                                               "reference build (oracle/_ref)"}))
-        return
-    with ThreadPoolExecutor(max(1, min(threads, 32))) as ex:
-        parts = list(ex.map(lambda c0: keygen.build_keys(min(chunk, n_build - c0), SEED, start=c0),
-                            range(0, n_build, chunk)))
-        bk = np.concatenate(parts)
-        if args.workload in CUCKOO_WORKLOADS:
-            assert f.insert(words, bk), "reference cuckoo build failed"   # its inserts are not thread-safe
-        elif z == 1:
-            f.insert_mt(words, bk, threads)
+        if args.workload in CLASSIC_WORKLOADS:
+            ck, ln, bpk, lp, hit, cmagic = CLASSIC_WORKLOADS[args.workload]
+            ref, m, fcfg = O.try_refcbf(), (1 << ln) * bpk, ("classic", ck, cmagic)
         else:
-            f.insert(words, bk)
-        del bk, parts
-        # probe sample: as many keys as take ~2 s per step on this host
+            bb, t, a, ln, lm, lp, hit = BCF_WORKLOADS[args.workload]
+            ref, m, fcfg = bcf_reference(), 1 << lm, ("bcf", bb, t, a)
+        if ref is None:
+            return unavailable("oracle/_ref (the reference compiled from its sources) is not built here")
+        f = ref.create(ck, m, cmagic) if fcfg[0] == "classic" else ref.create(m, bb, t, a)
+        words_u32 = f.alloc()
+        n_build, P = 1 << ln, 1 << lp
+        for c0 in range(0, n_build, chunk):   # their inserts are not atomic: one thread
+            f.insert(words_u32, keygen.build_keys(min(chunk, n_build - c0), SEED, start=c0))
+        words = np.zeros((len(words_u32) + 1) // 2 + 8, dtype=np.uint64)
+        words.view(np.uint32)[: len(words_u32)] = words_u32
+    else:
+        ref = O.try_reflib()
+        if ref is None:
+            return unavailable("oracle/_ref (the reference compiled from its sources) is not built here")
+        if args.workload in CUCKOO_WORKLOADS:
+            t, b, ln, lf, lp, hit = CUCKOO_WORKLOADS[args.workload]
+            m = cuckoo_bits(1 << ln, t, b, lf)
+            f, fcfg, wbytes = ref.cuckoo(t, b, m), ("cuckoo", t, b), 4
+        else:
+            wb, w, s, z, k, ln, bpk, lp, hit = WORKLOADS[args.workload]
+            m = (1 << ln) * bpk
+            f, fcfg, wbytes = ref.bloom(wb, w, s, z, k, m), (wb, w, s, z, k), wb
+        if f is None:
+            return unavailable("this configuration is not instantiated in the reference build (oracle/_ref)")
+        n_build, P = 1 << ln, 1 << lp
+        # filter words plus (cuckoo) the victim record the reference keeps after them
+        words = np.zeros((f.word_cnt * wbytes + 64) // 8, dtype=np.uint64)
+        with ThreadPoolExecutor(max(1, min(threads, 32))) as ex:
+            bk = np.concatenate(list(ex.map(lambda c0: keygen.build_keys(min(chunk, n_build - c0), SEED, start=c0),
+                                            range(0, n_build, chunk))))
+        if fcfg[0] == "cuckoo":
+            assert f.insert(words, bk), "reference cuckoo build failed"   # its inserts are not thread-safe
+        elif fcfg[3] == 1:
+            f.insert_mt(words, bk, threads)    # CAS-based, thread-safe (..._sgew.hpp:300-325)
+        else:
+            f.insert(words, bk)                # zoned inserts are not atomic
+        del bk
+    with ThreadPoolExecutor(max(1, min(threads, 32))) as ex:
         probe = np.concatenate(list(ex.map(
             lambda c0: keygen.probe_keys(n_build, min(chunk, P - c0), hit, SEED, start=c0)[0],
-            range(0, min(P, 1 << 26), chunk))))
-    out = np.empty(len(probe) + 64, dtype=np.uint32)
-    t0 = time.perf_counter()
-    f.batch_contains_mt(words, probe[:1 << 22], threads, unroll=1, out=out)
-    rate0 = (1 << 22) / max(1e-6, time.perf_counter() - t0)
-    n = int(min(len(probe), max(1 << 22, rate0 * 2.0)))
-    for _ in range(max(1, args.warmup)):
-        f.batch_contains_mt(words, probe[:n], threads, unroll=1, out=out)
-    times = []
-    cnt = 0
-    for _ in range(args.steps):
-        t0 = time.perf_counter()
-        cnt = f.batch_contains_mt(words, probe[:n], threads, unroll=1, out=out)
-        times.append(time.perf_counter() - t0)
-    ms = 1e3 * statistics.mean(times)
-    value = n / (ms / 1e3) / 1e9
+            range(0, min(P, REF_SAMPLE), chunk))))
+    rp = RefProbe(fcfg, m, words, threads)
+    rate, n, cnt, sec = rp.rate(probe, runs=args.steps, warmup=args.warmup)
+    value = rate / 1e9
     print(json.dumps({
         "impl": "reference", "metric": "probe Gkeys/s (batch_contains, ascending match positions)",
         "value": round(value, 4), "unit": "Gkeys/s", "n_gpus": world, "steps": args.steps,
-        "warmup": args.warmup, "ms_per_step": round(ms, 3), "higher_is_better": True, "scaling": "weak",
+        "warmup": args.warmup, "ms_per_step": round(sec * 1e3, 3), "higher_is_better": True, "scaling": "weak",
         "vs_baseline": None, "dtype": "u32", "data": "synthetic: seeded u32 bijection keys",
         "config": workload_config(args.workload, world),
         "cpu_baseline": {"value": round(value, 4), "unit": "Gkeys/s", "cores": threads, "kind": "reference",
-                         "sample": f"{n} of the workload's probe keys per step, {threads} threads x 1024-key "
-                                   f"batches (model/benchmark.cpp:123-165), SIMD batch_contains "
-                                   f"({ref.variant}, {ref.lanes} lanes)", "match_count": int(cnt)},
-        "e2e": {"value": round(value, 4), "unit": "Gkeys/s", "h2d_bytes_per_step": 0, "d2h_bytes_per_step": 0},
-    }), flush=True)
-
-
-def run_reference_bcf(args, threads, chunk):
-    """--impl reference for the blocked cuckoo and classic Bloom workloads: the
-    reference's dtl::bcf (bcf.cpp compiled from its sources) or
-    bloomfilter_logic (its header, instantiated), built by one thread (their
-    inserts are not atomic), probed by all host threads."""
-    import numpy as np
-
-    from dtlg import keygen
-    world = int(os.environ.get("WORLD_SIZE", "1"))
-    if args.workload in CLASSIC_WORKLOADS:
-        sys.path.insert(0, os.path.join(ROOT, "oracle"))
-        import oracle as O
-        ref = O.try_refcbf()
-        what = "oracle/_ref/libdtlref_cbf.so (the reference's bloomfilter_logic)"
-    else:
-        ref = bcf_reference()
-        what = "oracle/_ref/libdtlref_bcf*.so (the reference's dtl::bcf)"
-    if ref is None:
-        print(json.dumps({"impl": "reference", "unavailable": f"{what} is not built on this machine"}))
-        return
-    if args.workload in CLASSIC_WORKLOADS:
-        k, ln, bpk, lp, hit, magic = CLASSIC_WORKLOADS[args.workload]
-        f = ref.create(k, (1 << ln) * bpk, magic)
-        variant, api = "scalar", "bloomfilter_logic batch_contains"
-    else:
-        bb, t, a, ln, lm, lp, hit = BCF_WORKLOADS[args.workload]
-        f = ref.create(1 << lm, bb, t, a)
-        variant, api = ref.variant, "dtl::bcf batch_contains"
-    n_build, P = 1 << ln, 1 << lp
-    words = f.alloc()
-    for c0 in range(0, n_build, chunk):
-        f.insert(words, keygen.build_keys(min(chunk, n_build - c0), SEED, start=c0))
-    probe = np.concatenate([keygen.probe_keys(n_build, min(chunk, P - c0), hit, SEED, start=c0)[0]
-                            for c0 in range(0, min(P, 1 << 26), chunk)])
-    out = np.empty(len(probe) + 64, dtype=np.uint32)
-    t0 = time.perf_counter()
-    f.batch_contains_mt(words, probe[:1 << 22], threads, out=out)
-    rate0 = (1 << 22) / max(1e-6, time.perf_counter() - t0)
-    n = int(min(len(probe), max(1 << 22, rate0 * 2.0)))
-    for _ in range(max(1, args.warmup)):
-        f.batch_contains_mt(words, probe[:n], threads, out=out)
-    times = []
-    cnt = 0
-    for _ in range(args.steps):
-        t0 = time.perf_counter()
-        cnt = f.batch_contains_mt(words, probe[:n], threads, out=out)
-        times.append(time.perf_counter() - t0)
-    ms = 1e3 * statistics.mean(times)
-    value = n / (ms / 1e3) / 1e9
-    print(json.dumps({
-        "impl": "reference", "metric": "probe Gkeys/s (batch_contains, ascending match positions)",
-        "value": round(value, 4), "unit": "Gkeys/s", "n_gpus": world, "steps": args.steps,
-        "warmup": args.warmup, "ms_per_step": round(ms, 3), "higher_is_better": True, "scaling": "weak",
-        "vs_baseline": None, "dtype": "u32", "data": "synthetic: seeded u32 bijection keys",
-        "config": workload_config(args.workload, world),
-        "cpu_baseline": {"value": round(value, 4), "unit": "Gkeys/s", "cores": threads, "kind": "reference",
-                         "sample": f"{n} of the workload's probe keys per step, {threads} threads x 1024-key "
-                                   f"batches (model/benchmark.cpp:123-165), {api} "
-                                   f"({variant} build)", "match_count": int(cnt)},
+                         "sample": f"first {n} probe keys of this workload per step, mean over the steps, "
+                                   + rp.describe(),
+                         "unroll": rp.unroll, "unroll_ns_per_key": rp.unroll_ns, "match_count": cnt},
         "e2e": {"value": round(value, 4), "unit": "Gkeys/s", "h2d_bytes_per_step": 0, "d2h_bytes_per_step": 0},
     }), flush=True)
 
@@ -777,9 +781,14 @@ def batched_plan(n_filters=512, seed=4242, max_log2=24):
 
 
 def run_batched(args):
+    print(json.dumps(batched_bench(args)), flush=True)
+
+
+def batched_bench(args):
     """512 independent filters (zoned / sectorized, sizes log-uniform up to
     2^24) built and probed in one persistent, graph-captured launch vs the
-    same work as separate per-filter calls."""
+    same work as separate per-filter calls.  Both arms must give the same
+    filter words and the same match lists, bit for bit."""
     import ctypes as C
 
     import torch
@@ -848,16 +857,23 @@ def run_batched(args):
         torch.cuda.synchronize()
         return a.elapsed_time(b) / steps
 
-    # results of the two paths must agree
+    # results of the two paths must agree bit for bit: every filter's words
+    # and every match list
     per_filter_step()
     torch.cuda.synchronize()
+    ref_arena = arena.clone()
     ref_counts = [int(it.match_cnt.item()) for it in items]
-    ref_sums = [int(it.match_positions[:c].to(torch.int64).sum().item()) for it, c in zip(items, ref_counts)]
+    ref_lists = [it.match_positions[:c].clone() for it, c in zip(items, ref_counts)]
+    for it in items:
+        it.match_positions.fill_(-1)
+        it.match_cnt.fill_(-1)
     batched_step()
     torch.cuda.synchronize()
-    for it, c, sm in zip(items, ref_counts, ref_sums):
+    assert torch.equal(arena, ref_arena), "batched filter words differ from the per-filter build"
+    for it, c, lst in zip(items, ref_counts, ref_lists):
         assert int(it.match_cnt.item()) == c
-        assert int(it.match_positions[:c].to(torch.int64).sum().item()) == sm
+        assert torch.equal(it.match_positions[:c], lst)
+    del ref_arena, ref_lists
     steps = max(3, min(args.steps, 20))
     clocks = ClockSampler(int(os.environ.get("LOCAL_RANK", "0")))
     clocks.start()
@@ -886,9 +902,10 @@ def run_batched(args):
         "fallback_filters": batch.fallback_count(),
         "autotuned": {"staging": tuned["staging"], "ctas_per_sm": tuned["ctas_per_sm"],
                       "staged_filters": batch.staged_count()},
+        "bit_exact_vs_per_filter": True,
         "clocks": clk,
     }
-    print(json.dumps(result), flush=True)
+    return result
 
 
 def main():

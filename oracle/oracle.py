@@ -12,6 +12,7 @@ bench.py's CPU-baseline / reference legs, never by the product package.
 """
 import ctypes as C
 import os
+import time
 
 import numpy as np
 
@@ -379,6 +380,8 @@ class RefLib:
         L.ref_batch_contains_mt.restype = C.c_uint64
         L.ref_batch_contains_mt.argtypes = [vp, vp, _u32p, C.c_uint64, _u32p, C.c_int, C.c_int]
         L.ref_insert_mt.argtypes = [vp, vp, _u32p, C.c_uint64, C.c_int]
+        L.ref_batch_contains_mt_list.restype = C.c_uint64
+        L.ref_batch_contains_mt_list.argtypes = [vp, vp, _u32p, C.c_uint64, _u32p, C.c_int, C.c_int]
         L.ref_next_cheap_magic.restype = C.c_int
         L.ref_next_cheap_magic.argtypes = [C.c_uint32] + [C.POINTER(C.c_uint32)] * 3
         self.L = L
@@ -441,8 +444,45 @@ class _RefFilter:
             out = np.zeros(len(k) + 16, dtype=np.uint32)
         return self.ref.L.ref_batch_contains_mt(self.h, data.ctypes.data, k, len(k), out, threads, unroll)
 
+    def batch_contains_mt_list(self, data, keys, threads, unroll=1, out=None):
+        """All host threads, each on its own contiguous slice in 1024-key
+        batches, then the slices' lists joined: the ascending positions
+        (match_offset 0) of every matching key.  Returns a view of `out`."""
+        k = _keys(keys)
+        if out is None:
+            out = np.zeros(len(k) + 64, dtype=np.uint32)
+        n = self.ref.L.ref_batch_contains_mt_list(self.h, data.ctypes.data, k, len(k), out, threads, unroll)
+        return out[:n]
+
     def count_occupied(self, data):
         return self.ref.L.ref_count_occupied(self.h, data.ctypes.data)
+
+    def calibrate_unroll(self, words, cuckoo=False, min_s=0.25, seed=1):
+        """The reference's unroll choice (blocked_bloomfilter_tune_impl.hpp:
+        162-256; cuckoofilter_tune_impl.hpp:118-225): for u = 0, 1, 2, 4 (and 8
+        for cuckoo filters), probe 32 Ki uniform random keys in 1024-key batches
+        on one thread, repeatedly for at least 250 ms, against a zeroed filter
+        of the same size (the reference does not insert before timing), and
+        keep the u of the fewest time units per lookup.  `words` is the
+        filter's word array; a zeroed copy of its size is timed.  Returns
+        (u, {u: ns per lookup})."""
+        rng = np.random.default_rng(seed)
+        keys = rng.integers(0, 1 << 32, size=4 * 1024 * 8, dtype=np.uint64).astype(np.uint32)
+        zero = np.zeros_like(words)
+        zero[:] = 0   # touch the pages, as the reference's std::vector(size, 0) does
+        out = np.zeros(len(keys) + 64, dtype=np.uint32)
+        per = {}
+        for u in ((0, 1, 2, 4, 8) if cuckoo else (0, 1, 2, 4)):
+            reps = 0
+            t0 = time.perf_counter()
+            while True:
+                self.ref.L.ref_batch_contains_mt(self.h, zero.ctypes.data, keys, len(keys), out, 1, u)
+                reps += 1
+                dt = time.perf_counter() - t0
+                if dt > min_s:
+                    break
+            per[u] = dt * 1e9 / (reps * len(keys))
+        return min(per, key=per.get), per
 
 
 def try_reflib():
@@ -481,6 +521,8 @@ class RefBcf:
         L.ref_bcf_batch_contains.argtypes = [vp, vp, _u32p, C.c_uint32, _u32p, C.c_uint32]
         L.ref_bcf_batch_contains_mt.restype = C.c_uint64
         L.ref_bcf_batch_contains_mt.argtypes = [vp, vp, _u32p, C.c_uint64, _u32p, C.c_int]
+        L.ref_bcf_batch_contains_mt_list.restype = C.c_uint64
+        L.ref_bcf_batch_contains_mt_list.argtypes = [vp, vp, _u32p, C.c_uint64, _u32p, C.c_int]
         self.L = L
 
     def create(self, m, block_bytes=64, t=16, a=4):
@@ -535,6 +577,15 @@ class _RefBcfFilter:
             out = np.zeros(len(k) + 16, dtype=np.uint32)
         return self.ref.L.ref_bcf_batch_contains_mt(self.h, data.ctypes.data, k, len(k), out, threads)
 
+    def batch_contains_mt_list(self, data, keys, threads, out=None):
+        """batch_contains_mt, then the threads' slices joined: the ascending
+        positions (match_offset 0) of every matching key, a view of `out`."""
+        k = _keys(keys)
+        if out is None:
+            out = np.zeros(len(k) + 16, dtype=np.uint32)
+        n = self.ref.L.ref_bcf_batch_contains_mt_list(self.h, data.ctypes.data, k, len(k), out, threads)
+        return out[:n]
+
 
 def try_refbcf(variant="scalar"):
     try:
@@ -569,6 +620,8 @@ class RefCbf:
         L.ref_cbf_batch_contains.argtypes = [vp, vp, _u32p, C.c_uint32, _u32p, C.c_uint32]
         L.ref_cbf_batch_contains_mt.restype = C.c_uint64
         L.ref_cbf_batch_contains_mt.argtypes = [vp, vp, _u32p, C.c_uint64, _u32p, C.c_int]
+        L.ref_cbf_batch_contains_mt_list.restype = C.c_uint64
+        L.ref_cbf_batch_contains_mt_list.argtypes = [vp, vp, _u32p, C.c_uint64, _u32p, C.c_int]
         self.L = L
 
     def create(self, k, m, magic=False):
@@ -612,6 +665,15 @@ class _RefCbfFilter:
         if out is None:
             out = np.zeros(len(k) + 16, dtype=np.uint32)
         return self.ref.L.ref_cbf_batch_contains_mt(self.h, data.ctypes.data, k, len(k), out, threads)
+
+    def batch_contains_mt_list(self, data, keys, threads, out=None):
+        """batch_contains_mt, then the threads' slices joined: the ascending
+        positions (match_offset 0) of every matching key, a view of `out`."""
+        k = _keys(keys)
+        if out is None:
+            out = np.zeros(len(k) + 16, dtype=np.uint32)
+        n = self.ref.L.ref_cbf_batch_contains_mt_list(self.h, data.ctypes.data, k, len(k), out, threads)
+        return out[:n]
 
 
 def try_refcbf():

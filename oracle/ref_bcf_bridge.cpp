@@ -79,4 +79,34 @@ uint64_t ref_bcf_batch_contains_mt(void* h, const uint32_t* data, const uint32_t
   return total;
 }
 
+// As above, then the slices' lists moved together into the one ascending
+// list (positions i) that a single batch_contains over all n keys returns.
+uint64_t ref_bcf_batch_contains_mt_list(void* h, const uint32_t* data, const uint32_t* keys, uint64_t n,
+                                   uint32_t* out, int threads) {
+  dtl::bcf* f = static_cast<dtl::bcf*>(h);
+  if (threads < 1) threads = 1;
+  std::vector<uint64_t> cnt(threads, 0);
+  std::vector<std::thread> th;
+  for (int t = 0; t < threads; t++) {
+    th.emplace_back([=, &cnt]() {
+      const uint64_t b = n * (uint64_t)t / (uint64_t)threads;
+      const uint64_t e = n * (uint64_t)(t + 1) / (uint64_t)threads;
+      uint64_t c = 0;
+      for (uint64_t i = b; i < e; i += 1024) {
+        const uint32_t len = (uint32_t)std::min<uint64_t>(1024, e - i);
+        c += f->batch_contains(data, keys + i, len, out + b + c, (uint32_t)i);
+      }
+      cnt[t] = c;
+    });
+  }
+  for (auto& x : th) x.join();
+  uint64_t total = 0;
+  for (int t = 0; t < threads; t++) {
+    const uint64_t b = n * (uint64_t)t / (uint64_t)threads;
+    if (total != b && cnt[t]) std::memmove(out + total, out + b, cnt[t] * sizeof(uint32_t));
+    total += cnt[t];
+  }
+  return total;
+}
+
 }  // extern "C"

@@ -133,6 +133,38 @@ uint64_t ref_batch_contains_mt(void* h, const void* data, const uint32_t* keys, 
   return total;
 }
 
+// As ref_batch_contains_mt, then the threads' lists moved together: thread t
+// probed slice [b_t, e_t) and wrote its c_t positions at out + b_t, so moving
+// the slices down in thread order gives the one ascending list a single
+// batch_contains over all n keys returns (positions i, no offset).
+uint64_t ref_batch_contains_mt_list(void* h, const void* data, const uint32_t* keys, uint64_t n,
+                                    uint32_t* out, int threads, int unroll) {
+  handle* x = static_cast<handle*>(h);
+  if (threads < 1) threads = 1;
+  std::vector<uint64_t> cnt(threads, 0);
+  std::vector<std::thread> th;
+  for (int t = 0; t < threads; t++) {
+    th.emplace_back([=, &cnt]() {
+      const uint64_t b = n * (uint64_t)t / (uint64_t)threads;
+      const uint64_t e = n * (uint64_t)(t + 1) / (uint64_t)threads;
+      uint64_t c = 0;
+      for (uint64_t i = b; i < e; i += 1024) {
+        const uint32_t len = (uint32_t)std::min<uint64_t>(1024, e - i);
+        c += x->o->batch_contains(x->logic, data, keys + i, len, out + b + c, (uint32_t)i, unroll);
+      }
+      cnt[t] = c;
+    });
+  }
+  for (auto& t : th) t.join();
+  uint64_t total = 0;
+  for (int t = 0; t < threads; t++) {
+    const uint64_t b = n * (uint64_t)t / (uint64_t)threads;
+    if (total != b && cnt[t]) std::memmove(out + total, out + b, cnt[t] * sizeof(uint32_t));
+    total += cnt[t];
+  }
+  return total;
+}
+
 // Multi-threaded Bloom build: the sgew/sltw inserts are CAS-based and may run
 // concurrently (blocked_bloomfilter_block_logic_sgew.hpp:300-325).
 void ref_insert_mt(void* h, void* data, const uint32_t* keys, uint64_t n, int threads) {

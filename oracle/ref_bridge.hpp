@@ -118,8 +118,13 @@ struct cuckoo_ops {
                                  uint32_t* out, uint32_t off, int unroll) {
     const L* l = static_cast<L*>(p);
     const word_t* d = static_cast<const word_t*>(data);
+    // the unroll factors of the reference's cuckoo tuner, u in {0,1,2,4,8}
+    // (cuckoofilter_tune_impl.hpp:50,149)
     switch (unroll) {
       case 0: return l->batch_contains_scalar(d, keys, n, out, off);
+      case 2: return l->template batch_contains<kLanes * 2>(d, keys, n, out, off);
+      case 4: return l->template batch_contains<kLanes * 4>(d, keys, n, out, off);
+      case 8: return l->template batch_contains<kLanes * 8>(d, keys, n, out, off);
       default: return l->template batch_contains<kLanes>(d, keys, n, out, off);
     }
   }

@@ -6,6 +6,7 @@
 // header is included from its place in the reference tree (oracle/Makefile
 // sets the include path) and instantiated for both addressing modes, as a
 // user of that header-only template does.  Its batch_contains is scalar.
+#include <cstring>
 #include <cstdint>
 #include <thread>
 #include <vector>
@@ -93,6 +94,35 @@ uint64_t ref_cbf_batch_contains_mt(void* v, const uint32_t* data, const uint32_t
   uint64_t total = 0;
   for (int t = 0; t < threads; t++) {
     th[t].join();
+    total += cnt[t];
+  }
+  return total;
+}
+
+// As above, then the slices' lists moved together into the one ascending
+// list (positions i) that a single batch_contains over all n keys returns.
+uint64_t ref_cbf_batch_contains_mt_list(void* v, const uint32_t* data, const uint32_t* keys, uint64_t n,
+                                   uint32_t* out, int threads) {
+  if (threads < 1) threads = 1;
+  std::vector<uint64_t> cnt(threads, 0);
+  std::vector<std::thread> th;
+  for (int t = 0; t < threads; t++) {
+    th.emplace_back([=, &cnt]() {
+      const uint64_t b = n * (uint64_t)t / (uint64_t)threads;
+      const uint64_t e = n * (uint64_t)(t + 1) / (uint64_t)threads;
+      uint64_t c = 0;
+      for (uint64_t i = b; i < e; i += 1024) {
+        const uint32_t len = (uint32_t)std::min<uint64_t>(1024, e - i);
+        c += ref_cbf_batch_contains(v, data, keys + i, len, out + b + c, (uint32_t)i);
+      }
+      cnt[t] = c;
+    });
+  }
+  for (auto& x : th) x.join();
+  uint64_t total = 0;
+  for (int t = 0; t < threads; t++) {
+    const uint64_t b = n * (uint64_t)t / (uint64_t)threads;
+    if (total != b && cnt[t]) std::memmove(out + total, out + b, cnt[t] * sizeof(uint32_t));
     total += cnt[t];
   }
   return total;
