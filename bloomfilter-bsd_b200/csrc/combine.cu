@@ -1,4 +1,5 @@
-// combine.cu -- OR-combines partial Bloom filters (sharded builds).
+// combine.cu -- OR-combines partial Bloom filters (sharded builds), and
+// copies filter words between devices (per-device replicas).
 //
 // A Bloom build sharded over G GPUs inserts each GPU's share of the keys into
 // its own copy of the filter words; OR is the only reduction the words need,
@@ -41,6 +42,18 @@ dtlg_status dtlg_or_words(uint64_t* dst, const uint64_t* src, uint64_t n_words, 
   const unsigned grid = static_cast<unsigned>(blocks < static_cast<uint64_t>(sms) * 8 ? blocks : sms * 8ull);
   or_words_kernel<<<grid, 256, 0, reinterpret_cast<cudaStream_t>(stream)>>>(dst, src, n_words, n_src, src_stride);
   DTLG_TRY_CUDA(cudaGetLastError());
+  return DTLG_OK;
+}
+
+// A copy engine transfer (cudaMemcpyPeerAsync): no kernel of this library or
+// of any other reads the other device's memory.
+dtlg_status dtlg_copy_words_peer(uint64_t* dst, int dst_device, const uint64_t* src, int src_device,
+                                 uint64_t n_words, dtlg_stream_t stream) {
+  if (n_words == 0) return DTLG_OK;
+  if (!dst || !src) return DTLG_ERR_NULL;
+  if (dst_device < 0 || src_device < 0) return DTLG_ERR_INVALID_CONFIG;
+  DTLG_TRY_CUDA(cudaMemcpyPeerAsync(dst, dst_device, src, src_device, n_words * sizeof(uint64_t),
+                                    reinterpret_cast<cudaStream_t>(stream)));
   return DTLG_OK;
 }
 

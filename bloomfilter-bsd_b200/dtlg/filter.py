@@ -14,6 +14,7 @@ with the reference.  Errors raise: InvalidConfig / SizeError mirror the
 reference's std::invalid_argument / std::logic_error.
 """
 import ctypes as C
+import threading
 from dataclasses import dataclass
 
 import numpy as np
@@ -345,17 +346,69 @@ def construct(config, m):
     raise _lib.InvalidConfig(1, "Illegal configuration. Word size must be either 4 or 8.")
 
 
+class DeviceReplicas:
+    """The filter words once per device, each copy made on first use.
+
+    The GPU counterpart of the reference's per-NUMA-node replicas
+    (filter.hpp:98-101,128-152): the words live on the device that built them
+    (`home`); the first probe from another device copies them there, under a
+    lock with a second check, as the reference does per memory node.  `copy`
+    makes one replica: copy(home_words, device) -> words on that device.  An
+    insert makes every replica stale, so invalidate() drops them (the
+    reference leaves inserting after probing undefined, filter.hpp:33-34).
+    """
+
+    def __init__(self, words, home, copy):
+        self.home = home
+        self._words = {home: words}
+        self._copy = copy
+        self._lock = threading.Lock()
+
+    def get(self, device):
+        w = self._words.get(device)
+        if w is not None:
+            return w
+        with self._lock:
+            w = self._words.get(device)
+            if w is None:                      # double check, as filter.hpp:139-147
+                w = self._copy(self._words[self.home], device)
+                self._words[device] = w
+        return w
+
+    def devices(self):
+        return sorted(self._words)
+
+    def invalidate(self):
+        with self._lock:
+            self._words = {self.home: self._words[self.home]}
+
+
+def _peer_replica(words, device):
+    """A copy of the filter words on `device`: a copy-engine transfer
+    (dtlg_copy_words_peer), no kernel reads the other device's memory."""
+    torch = _torch()
+    dst = torch.empty(words.numel(), dtype=words.dtype, device=torch.device("cuda", device))
+    with torch.cuda.device(device):
+        st = lib().dtlg_copy_words_peer(C.c_void_p(dst.data_ptr()), device, C.c_void_p(words.data_ptr()),
+                                        words.device.index, words.numel(), _stream())
+        check(st, "dtlg_copy_words_peer")
+        torch.cuda.current_stream().synchronize()
+    return dst
+
+
 class filter:  # noqa: N801 -- dtl::filter::filter (filter.hpp:35-261)
     """Construct by config, insert, then probe through probe instances.
 
     As in the reference, insert() must not be called after probe() handed out
-    a probe instance (filter.hpp:33-34).  The filter words live on one CUDA
-    device (the reference's NUMA replication has no single-GPU counterpart).
+    a probe instance (filter.hpp:33-34); here it drops the replicas.  The
+    words are built on one CUDA device and replicated to every other device
+    that probes them (DeviceReplicas).
     """
 
     def __init__(self, config, m, device="cuda"):
         self.filter_instance = construct(config, m)
         self.filter_data = self.filter_instance.alloc_filter_data(device)
+        self.replicas = DeviceReplicas(self.filter_data, self.filter_data.device.index, _peer_replica)
 
     @staticmethod
     def for_workload(n, work_ns, fpr_target=0.1, hit_ratio=0.0, l2_resident=False, method="mlp", device="cuda"):
@@ -370,28 +423,49 @@ class filter:  # noqa: N801 -- dtl::filter::filter (filter.hpp:35-261)
 
     def insert(self, keys):
         torch = _torch()
-        if isinstance(keys, torch.Tensor) and keys.is_cuda:
-            return self.filter_instance.batch_insert(self.filter_data, keys)
-        return self.filter_instance.batch_insert_host(self.filter_data, np.asarray(keys, dtype=np.uint32))
+        self.replicas.invalidate()
+        with torch.cuda.device(self.filter_data.device):
+            if isinstance(keys, torch.Tensor) and keys.is_cuda:
+                keys = keys.to(self.filter_data.device)
+                return self.filter_instance.batch_insert(self.filter_data, keys)
+            return self.filter_instance.batch_insert_host(self.filter_data, np.asarray(keys, dtype=np.uint32))
+
+    def filter_data_on(self, device):
+        """The words on `device` (an index), replicated there on first use
+        (filter_shared::get_filter_data_ptr, filter.hpp:128-152)."""
+        return self.replicas.get(device)
 
     def probe(self):
         return probe_t(self)
 
 
 class probe_t:  # noqa: N801 -- filter.hpp:205-253
+    """Probes against the replica on the device of the keys (host keys: the
+    current device).  The reference's probe_t fetches its node's replica
+    (filter.hpp:212-215) but then probes the original words
+    (filter.hpp:234-240); here the replica is the one probed."""
+
     def __init__(self, f):
         self._f = f
+
+    def device_of(self, keys):
+        torch = _torch()
+        if isinstance(keys, torch.Tensor) and keys.is_cuda:
+            return keys.device.index
+        return torch.cuda.current_device()
 
     def __call__(self, keys, match_pos=None, match_offset=0):
         """Returns the match count; positions go to match_pos (a CUDA tensor
         for device keys, a numpy uint32 array for host keys)."""
         torch = _torch()
-        fi, data = self._f.filter_instance, self._f.filter_data
-        if isinstance(keys, torch.Tensor) and keys.is_cuda:
+        dev = self.device_of(keys)
+        fi, data = self._f.filter_instance, self._f.filter_data_on(dev)
+        with torch.cuda.device(dev):
+            if isinstance(keys, torch.Tensor) and keys.is_cuda:
+                if match_pos is None:
+                    match_pos = torch.empty(max(1, keys.numel()), dtype=torch.int32, device=keys.device)
+                return fi.batch_contains(data, keys.contiguous(), keys.numel(), match_pos, match_offset)
+            keys = np.ascontiguousarray(keys, dtype=np.uint32)
             if match_pos is None:
-                match_pos = torch.empty(max(1, keys.numel()), dtype=torch.int32, device=keys.device)
-            return fi.batch_contains(data, keys.contiguous(), keys.numel(), match_pos, match_offset)
-        keys = np.ascontiguousarray(keys, dtype=np.uint32)
-        if match_pos is None:
-            match_pos = np.empty(max(1, keys.size), dtype=np.uint32)
-        return fi.batch_contains_host(data, keys, match_pos, match_offset)
+                match_pos = np.empty(max(1, keys.size), dtype=np.uint32)
+            return fi.batch_contains_host(data, keys, match_pos, match_offset)

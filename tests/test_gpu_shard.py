@@ -40,3 +40,44 @@ def test_partial_builds_or_to_the_full_build():
     combined = parts[0].clone()
     or_words(combined, parts[1:])
     assert torch.equal(combined, full)
+
+
+def test_facade_replica_path_returns_the_oracles_list():
+    """filter.probe() probes the replica of the keys' device.  On one GPU the
+    home words are that replica; the copy a second device would get
+    (dtlg_copy_words_peer, here device 0 -> device 0) is bit-identical and
+    probes to the same list, the oracle's."""
+    import importlib
+
+    import numpy as np
+    import oracle as O
+    from dtlg import keygen
+    Fm = importlib.import_module("dtlg.filter")
+    m = 12 * 100000 + 77
+    f = F.filter(F.blocked_bloomfilter_config(k=8, word_size=8, word_cnt_per_block=8, sector_cnt=8), m)
+    bk = keygen.build_keys(100000, 61)
+    assert f.insert(torch.from_numpy(bk.view(np.int32)).cuda())
+    ob = O.Bloom(8, 8, 8, 1, 8, m)
+    rw = ob.alloc()
+    ob.insert(rw, bk)
+    pk, _ = keygen.probe_keys(100000, 300000, 0.2, 61)
+    want = ob.batch_contains(rw, pk, 3)
+    keys = torch.from_numpy(pk.view(np.int32)).cuda()
+    p = f.probe()
+    out = torch.zeros(len(pk), dtype=torch.int32, device="cuda")
+    n = p(keys, out, 3)
+    assert np.array_equal(out[:n].cpu().numpy().view(np.uint32), want)
+    assert f.replicas.devices() == [0]                       # no copy for the home device
+    copy = Fm._peer_replica(f.filter_data, 0)
+    assert copy.data_ptr() != f.filter_data.data_ptr() and torch.equal(copy, f.filter_data)
+    out2 = torch.zeros(len(pk), dtype=torch.int32, device="cuda")
+    n2 = f.filter_instance.batch_contains(copy, keys, len(pk), out2, 3)
+    assert n2 == n and torch.equal(out2[:n2], out[:n])
+    # host keys go to the current device's replica
+    hp = np.zeros(len(pk), dtype=np.uint32)
+    assert p(pk, hp, 3) == n and np.array_equal(hp[:n], want)
+    if torch.cuda.device_count() > 1:
+        k1 = keys.to("cuda:1")
+        o1 = torch.zeros(len(pk), dtype=torch.int32, device="cuda:1")
+        assert p(k1, o1, 3) == n and np.array_equal(o1[:n].cpu().numpy().view(np.uint32), want)
+        assert f.replicas.devices() == [0, 1]
