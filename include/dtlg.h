@@ -193,7 +193,7 @@ dtlg_status dtlg_set_probe_options(dtlg_filter* f, int mode, int variant);
  * the reference, whose batch_insert is one loop): 0 = automatic (2 for Bloom
  * filters beyond 160 MiB and batches of >= 2^20 keys, else 1), 1 = one kernel of
  * global atomics, 2 = keys first grouped by ~8 MiB block range (the
- * partitioned probe's partition, 8 bytes per key of workspace from the
+ * partitioned probe's partition, ~8.3 bytes per key of workspace from the
  * library's stream-ordered pool; without room there, plan 1), then inserted
  * range by range so the atomics hit L2.  Bloom filter
  * words are the same under every plan; blocked cuckoo builds are randomised
@@ -379,6 +379,16 @@ dtlg_status dtlg_mlp_choose(dtlg_mlp* m, const float* x, uint32_t n, uint32_t n_
  * node (filter.hpp:128-152) and has no sharded build. */
 dtlg_status dtlg_or_words(uint64_t* dst, const uint64_t* src, uint64_t n_words, uint32_t n_src, uint64_t src_stride,
                           dtlg_stream_t stream);
+
+/* ---- per-device replicas (filter.hpp:98-152) ----
+ * Copies n_words filter words from src on src_device to dst on dst_device
+ * (device pointers; a copy-engine transfer enqueued on `stream`, which must
+ * belong to the current device).  The reference keeps one replica of the
+ * filter words per NUMA node, made on first use by a thread of that node
+ * (filter.hpp:128-152); the host mirror (dtlg.filter) keeps one per GPU the
+ * same way and probes each device's keys against its own replica. */
+dtlg_status dtlg_copy_words_peer(uint64_t* dst, int dst_device, const uint64_t* src, int src_device,
+                                 uint64_t n_words, dtlg_stream_t stream);
 
 /* ---- single keys: filter_base::insert / contains (filter_base.hpp:22,32) ---- */
 dtlg_status dtlg_insert(const dtlg_filter* f, uint64_t* filter_words, uint32_t key, dtlg_stream_t stream);
