@@ -8,8 +8,12 @@
 // lookup time read from GPU calibration runs (t per key at log2-spaced filter
 // sizes, linearly interpolated) instead of per-cache-level deltas:
 //
-//   cost(c, m) = t_c(m / 8 bytes) + ns_per_match * (h + (1 - h) * f)
+//   cost(c, m) = t_c(m / 8 bytes, f, h) + ns_per_match * (h + (1 - h) * f)
 //                + work_ns * (1 - h) * f,        f = fpr_c(m / n)
+//
+// where t_c is the first half of a block's probe plus, for the keys that go
+// on (members, and non-members passing the first half), the second half:
+// t_c = first_c(m) + (h + (1 - h) sqrt(f)) second_c(m).
 //
 // subject to f <= fpr_target and, for L2-resident queries, m / 8 <=
 // l2_budget_bytes.  Queries are split over host threads.
@@ -24,8 +28,8 @@
 
 namespace {
 
-double lookup_ns(const dtlg_cost_tables* t, uint32_t c, double log2_bytes) {
-  const double* row = t->ns_per_key + static_cast<size_t>(c) * t->n_size;
+double lookup_row(const dtlg_cost_tables* t, const double* table, uint32_t c, double log2_bytes) {
+  const double* row = table + static_cast<size_t>(c) * t->n_size;
   if (t->n_size == 1) return row[0];
   double x = (log2_bytes - t->log2_bytes_first) / t->log2_bytes_step;
   x = std::min(std::max(x, 0.0), static_cast<double>(t->n_size - 1));
@@ -33,6 +37,19 @@ double lookup_ns(const dtlg_cost_tables* t, uint32_t c, double log2_bytes) {
   if (i > t->n_size - 2) i = t->n_size - 2;
   const double f = x - i;
   return row[i] * (1.0 - f) + row[i + 1] * f;
+}
+
+// Probe time per key of candidate c at a filter of 2^log2_bytes bytes, for a
+// filter whose false-positive rate is f, at hit ratio h: the first half of the
+// block always, the second half for members and for the non-members that pass
+// the first half (probability sqrt(f)).
+double lookup_ns(const dtlg_cost_tables* t, uint32_t c, double log2_bytes, double f, double h) {
+  double ns = lookup_row(t, t->ns_per_key, c, log2_bytes);
+  if (t->ns_second) {
+    const double q = std::min(1.0, std::sqrt(std::max(0.0, f)));
+    ns += (h + (1.0 - h) * q) * lookup_row(t, t->ns_second, c, log2_bytes);
+  }
+  return ns;
 }
 
 void search_range(const dtlg_cost_tables* t, const dtlg_cost_query* q, uint32_t q0, uint32_t q1, double* cand_cost,
@@ -55,8 +72,8 @@ void search_range(const dtlg_cost_tables* t, const dtlg_cost_query* q, uint32_t 
         if (!(f <= Q.fpr_target)) continue;
         const double bytes = n * t->bits_per_key[k] / 8.0;
         if (Q.l2_resident && bytes > t->l2_budget_bytes) continue;
-        const double cost = lookup_ns(t, c, Q.log2_n + log2_bpk[k] - 3.0) + t->ns_per_match * (h + miss * f) +
-                            Q.work_ns * miss * f;
+        const double cost = lookup_ns(t, c, Q.log2_n + log2_bpk[k] - 3.0, f, h) +
+                            t->ns_per_match * (h + miss * f) + Q.work_ns * miss * f;
         if (cost < c_cost) {
           c_cost = cost;
           c_bpk = t->bits_per_key[k];
@@ -122,7 +139,8 @@ dtlg_status dtlg_cost_eval(const dtlg_cost_tables* t, const dtlg_cost_query* que
       continue;
     }
     const double miss = 1.0 - Q.hit_ratio;
-    cost[qi] = lookup_ns(t, static_cast<uint32_t>(c), Q.log2_n + std::log2(t->bits_per_key[k]) - 3.0) +
+    cost[qi] = lookup_ns(t, static_cast<uint32_t>(c), Q.log2_n + std::log2(t->bits_per_key[k]) - 3.0, f,
+                         Q.hit_ratio) +
                t->ns_per_match * (Q.hit_ratio + miss * f) + Q.work_ns * miss * f;
   }
   return DTLG_OK;

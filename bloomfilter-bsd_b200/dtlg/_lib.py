@@ -71,7 +71,8 @@ class BatchPlanS(C.Structure):
 class CostTablesS(C.Structure):
     _fields_ = [("n_cand", C.c_uint32), ("n_bpk", C.c_uint32), ("bits_per_key", C.c_void_p), ("fpr", C.c_void_p),
                 ("n_size", C.c_uint32), ("log2_bytes_first", C.c_double), ("log2_bytes_step", C.c_double),
-                ("ns_per_key", C.c_void_p), ("ns_per_match", C.c_double), ("l2_budget_bytes", C.c_double)]
+                ("ns_per_key", C.c_void_p), ("ns_per_match", C.c_double), ("l2_budget_bytes", C.c_double),
+                ("ns_second", C.c_void_p)]
 
 
 class CostQueryS(C.Structure):

@@ -7,13 +7,25 @@ the TLB reach near 256 MiB, HBM), so each candidate is timed directly on a
 grid of filter sizes and the cost model interpolates between grid points in
 log2(bytes).
 
-One run = one candidate at one size: a filter of that many bytes (zeroed; a
-probe's memory traffic does not depend on the bit contents, since every
-probe reads all of its words) probed with uniform random uint32 keys through
-the public batch_contains path, timed with CUDA events (median of `reps`
-launches after a warm-up).  A zeroed filter matches nothing; the cost of a
-match (writing its position) is measured separately on all-ones Bloom
-filters, where every key matches, and reported as ns_per_match.
+A probe tests the first half of a block (the first half of its words, or of
+its zones / sectors) and loads the second half only when the first passes;
+how often that happens depends on how full the filter is.  So every run
+times two fills of the same filter:
+
+* zeroed: every key fails on the first half -> ns_per_key, the first half;
+* half-filled: the first half of every block all ones, the second half
+  zeros -> every key passes the first half, loads the second and fails
+  there; the difference is ns_second, the cost of the second half.
+
+The cost model prices a filter at its bits per key from these two
+(cost.py).  Layouts without a second part (blocks of one word, fixed-word
+blocks under 64 bytes) show ns_second ~ 0.  Filters are probed with uniform
+random uint32 keys through the public batch_contains path, timed with CUDA
+events (median of `reps` launches after a warm-up).  The cost of a match
+(writing its position) is measured on all-ones Bloom filters, where every key
+matches, and reported as ns_per_match; the few keys a half-filled filter
+matches (a layout whose bits can all fall in the first half) are charged at
+that rate and taken out of ns_second.
 
     python -m dtlg.model.calibration --out calibration.npz   (needs a GPU)
 """
@@ -36,21 +48,24 @@ DEFAULT_PATH = os.path.join(DATA_DIR, "calibration_b200.npz")
 class CalibrationData:
     candidates: list            # [Candidate]
     log2_bytes: np.ndarray      # (S,) filter sizes of the grid
-    ns_per_key: np.ndarray      # (C, S) probe time per key, zero matches
+    ns_per_key: np.ndarray      # (C, S) probe time per key, zeroed filter (first half only)
     ns_per_match: float         # added cost per matching key
     meta: dict = field(default_factory=dict)
+    ns_second: np.ndarray = None  # (C, S) added time per key that loads the second half
 
     def save(self, path):
+        extra = {} if self.ns_second is None else {"ns_second": self.ns_second}
         np.savez_compressed(path, candidates=np.array([c.name for c in self.candidates]),
                             log2_bytes=self.log2_bytes, ns_per_key=self.ns_per_key,
-                            ns_per_match=np.float64(self.ns_per_match), meta=json.dumps(self.meta))
+                            ns_per_match=np.float64(self.ns_per_match), meta=json.dumps(self.meta), **extra)
 
     @staticmethod
     def load(path=DEFAULT_PATH):
         z = np.load(path, allow_pickle=False)
+        sec = z["ns_second"].astype(np.float64) if "ns_second" in z.files else None
         return CalibrationData([by_name(str(n)) for n in z["candidates"]], z["log2_bytes"].astype(np.float64),
                                z["ns_per_key"].astype(np.float64), float(z["ns_per_match"]),
-                               json.loads(str(z["meta"])))
+                               json.loads(str(z["meta"])), sec)
 
     def index(self, cand):
         return [c.name for c in self.candidates].index(cand.name)
@@ -104,9 +119,24 @@ class _Runner:
         return float(np.median(ts)), int(self.cnt.item())
 
 
+def _half_fill(arena, block_bytes):
+    """The first half of every block-sized stretch of the arena all ones, the
+    second half zeros (blocks of one word: all zeros)."""
+    import torch
+    b = arena.view(torch.uint8)
+    pat = torch.zeros(block_bytes, dtype=torch.uint8, device=arena.device)
+    if block_bytes >= 8:
+        pat[: block_bytes // 2] = 0xFF
+    reps = b.numel() // block_bytes
+    b[: reps * block_bytes].view(reps, block_bytes).copy_(pat.expand(reps, block_bytes))
+    b[reps * block_bytes:].zero_()
+
+
 def run_calibration(candidates=None, log2_bytes=DEFAULT_LOG2_BYTES, probe_cnt=1 << 23, reps=3, seed=2024,
                     device="cuda", progress=True):
-    """Time every candidate at every size; returns CalibrationData plus the run log."""
+    """Time every candidate at every size, zeroed and half-filled; returns
+    CalibrationData plus the run log (candidate, log2 bytes, m, ns zeroed, ns
+    second half)."""
     import torch
 
     from .. import construct
@@ -114,22 +144,8 @@ def run_calibration(candidates=None, log2_bytes=DEFAULT_LOG2_BYTES, probe_cnt=1 
     log2_bytes = np.asarray(log2_bytes, dtype=np.float64)
     max_bytes = max(_magic_bits(2.0 ** log2_bytes.max(), c) // 8 for c in candidates) + 4096
     R = _Runner(probe_cnt, max_bytes, seed, device)
-    t = np.zeros((len(candidates), len(log2_bytes)))
-    runs = []
     t_start = time.time()
-    for ci, cand in enumerate(candidates):
-        for si, lb in enumerate(log2_bytes):
-            m = _magic_bits(2.0 ** lb, cand)
-            f = construct(cand.config(), m)
-            words = R.arena[:max(1, f.alloc_words())]
-            ns, cnt = R.probe_ns_per_key(f, words, reps)
-            if cnt != 0:
-                raise RuntimeError(f"{cand.name}: zeroed filter matched {cnt} keys")
-            t[ci, si] = ns
-            runs.append((ci, float(lb), m, ns))
-        if progress and (ci % 16 == 15 or ci == len(candidates) - 1):
-            print(f"calibrated {ci + 1}/{len(candidates)} candidates, {time.time() - t_start:.0f} s", flush=True)
-    # the cost of a match: all-ones Bloom filters match every key
+    # the cost of a match first: all-ones Bloom filters match every key
     deltas = []
     blooms = [c for c in candidates if c.kind == "bloom"]
     for cand in blooms[::max(1, len(blooms) // 12)]:
@@ -143,13 +159,49 @@ def run_calibration(candidates=None, log2_bytes=DEFAULT_LOG2_BYTES, probe_cnt=1 
             ns0, _ = R.probe_ns_per_key(f, words, reps)
             assert cnt == probe_cnt
             deltas.append(ns1 - ns0)
+    ns_match = float(np.median(deltas))
+    t = np.zeros((len(candidates), len(log2_bytes)))
+    t2 = np.zeros((len(candidates), len(log2_bytes)))
+    runs = []
+    # zeroed runs
+    R.arena.zero_()
+    for ci, cand in enumerate(candidates):
+        for si, lb in enumerate(log2_bytes):
+            m = _magic_bits(2.0 ** lb, cand)
+            f = construct(cand.config(), m)
+            ns, cnt = R.probe_ns_per_key(f, R.arena[:max(1, f.alloc_words())], reps)
+            if cnt != 0:
+                raise RuntimeError(f"{cand.name}: zeroed filter matched {cnt} keys")
+            t[ci, si] = ns
+        if progress and (ci % 32 == 31 or ci == len(candidates) - 1):
+            print(f"zeroed: {ci + 1}/{len(candidates)} candidates, {time.time() - t_start:.0f} s", flush=True)
+    # half-filled runs, Bloom candidates grouped by block size (one fill each)
+    for bb in sorted({c.block_bytes for c in blooms}):
+        _half_fill(R.arena, bb)
+        for ci, cand in enumerate(candidates):
+            if cand.kind != "bloom" or cand.block_bytes != bb:
+                continue
+            for si, lb in enumerate(log2_bytes):
+                m = _magic_bits(2.0 ** lb, cand)
+                f = construct(cand.config(), m)
+                ns, cnt = R.probe_ns_per_key(f, R.arena[:max(1, f.alloc_words())], reps)
+                t2[ci, si] = max(0.0, ns - ns_match * cnt / probe_cnt - t[ci, si])
+        if progress:
+            print(f"half-filled: {bb}-byte blocks, {time.time() - t_start:.0f} s", flush=True)
+    R.arena.zero_()
+    for ci in range(len(candidates)):
+        for si, lb in enumerate(log2_bytes):
+            runs.append((ci, float(lb), _magic_bits(2.0 ** lb, candidates[ci]), t[ci, si], t2[ci, si]))
     props = torch.cuda.get_device_properties(R.dev)
     meta = {"device": props.name, "sms": props.multi_processor_count, "l2_bytes": getattr(props, "L2_cache_size", 0),
-            "probe_keys": probe_cnt, "reps": reps, "seed": seed, "runs": len(runs) + 2 * len(deltas),
+            "probe_keys": probe_cnt, "reps": reps, "seed": seed,
+            "runs": len(runs) + int(np.sum([c.kind == "bloom" for c in candidates])) * len(log2_bytes)
+            + 2 * len(deltas),
             "match_cost_runs": len(deltas), "api": "dtlg_batch_contains_ws (automatic probe plan)",
+            "fills": "zeroed (first half of each block) and half-filled (second half of each block)",
             "keys": "uniform random uint32 (torch.randint)", "seconds": round(time.time() - t_start, 1),
             "date": time.strftime("%Y-%m-%d")}
-    return CalibrationData(candidates, log2_bytes, t, float(np.median(deltas)), meta), np.array(runs)
+    return CalibrationData(candidates, log2_bytes, t, ns_match, meta, t2), np.array(runs)
 
 
 def main():

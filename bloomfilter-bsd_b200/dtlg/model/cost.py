@@ -2,11 +2,17 @@
 
 A query asks for the filter that minimises the cost per probed key
 
-    cost(c, bpk) = t_c(n * bpk / 8 bytes) + ns_per_match * (h + (1 - h) * f)
+    cost(c, bpk) = t_c(n * bpk / 8 bytes, f, h) + ns_per_match * (h + (1 - h) * f)
                    + work_ns * (1 - h) * f,            f = fpr_c(bpk),
 
+    t_c(size, f, h) = first_c(size) + (h + (1 - h) * sqrt(f)) * second_c(size),
+
 subject to f <= fpr_target and, for an L2-resident query, a filter of at most
-l2_budget_bytes.  t_c comes from the GPU calibration runs.  This is the
+l2_budget_bytes.  first_c and second_c come from the GPU calibration runs:
+the probe tests the first half of a block and loads the second half only for
+keys that pass it -- every member, and a non-member with probability about
+sqrt(f) -- so a filter with fewer bits per key (more bits set) pays the second
+half more often.  This is the
 reference's overhead = t_lookup(m) + tw * fpr(m, n, c) (model/cost_fn.hpp:
 150-160) minimised over m for every configuration (model/optimizer.hpp:25-140,
 tool/calibration/src/skyline_matrix_builder.cpp:88-115), with two query terms
@@ -87,6 +93,8 @@ class CostModel:
         self.bpk = np.ascontiguousarray(bpk_grid, dtype=np.float64)
         self.fpr = np.ascontiguousarray(np.stack([c.fpr(self.bpk) for c in self.candidates]), dtype=np.float64)
         self.ns = np.ascontiguousarray(calib.ns_per_key, dtype=np.float64)
+        self.ns_second = (None if calib.ns_second is None
+                          else np.ascontiguousarray(calib.ns_second, dtype=np.float64))
         lb = calib.log2_bytes
         step = float(lb[1] - lb[0]) if len(lb) > 1 else 1.0
         if len(lb) > 2 and not np.allclose(np.diff(lb), step, atol=1e-6):
@@ -94,7 +102,7 @@ class CostModel:
         self.l2_budget_bytes = float(l2_budget_bytes)
         self.tables = _lib.CostTablesS(len(self.candidates), len(self.bpk), _ptr(self.bpk), _ptr(self.fpr), len(lb),
                                        float(lb[0]), step, _ptr(self.ns), float(calib.ns_per_match),
-                                       self.l2_budget_bytes)
+                                       self.l2_budget_bytes, _ptr(self.ns_second))
 
     @property
     def n_cand(self):

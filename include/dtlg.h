@@ -324,6 +324,13 @@ typedef struct dtlg_cost_tables {
   const double* ns_per_key;     /* [C*S] probe time per key */
   double ns_per_match;          /* added time per matching key */
   double l2_budget_bytes;       /* size limit of l2_resident queries */
+  /* [C*S] added time per key that loads the second half of its block (the
+   * probe tests the first half first and skips the rest when it fails);
+   * NULL: no second part.  A key loads it when it is a member (h) or a
+   * non-member that passes the first half, q = sqrt(f) (the half's false-
+   * positive rate where both halves are alike; an upper bound otherwise):
+   *   t_c = ns_per_key + (h + (1 - h) q) ns_second */
+  const double* ns_second;
 } dtlg_cost_tables;
 typedef struct dtlg_cost_query {
   double log2_n;                /* build keys */

@@ -117,9 +117,11 @@ def lookup_ns(ns_row, first, step, log2_bytes):
     return ns_row[i] * (1.0 - f) + ns_row[i + 1] * f
 
 
-def search(bpk, fpr, first, step, ns, ns_per_match, budget, q):
+def search(bpk, fpr, first, step, ns, ns_per_match, budget, q, ns_second=None):
     """One query q = (log2_n, fpr_target, hit_ratio, work_ns, l2_resident):
-    (best index or -1, best cost, per-candidate best costs)."""
+    (best index or -1, best cost, per-candidate best costs).  ns_second: the
+    added time of a block's second half, paid by members and by the
+    non-members that pass the first half (probability sqrt(f))."""
     log2_n, target, h, work, l2 = q
     n = 2.0 ** log2_n
     best, best_cost, per = -1, math.inf, []
@@ -131,8 +133,11 @@ def search(bpk, fpr, first, step, ns, ns_per_match, budget, q):
                 continue
             if l2 and n * bpk[k] / 8.0 > budget:
                 continue
-            cost = (lookup_ns(ns[c], first, step, log2_n + math.log2(bpk[k]) - 3.0) + ns_per_match * (h + (1 - h) * f)
-                    + work * (1 - h) * f)
+            lb = log2_n + math.log2(bpk[k]) - 3.0
+            t = lookup_ns(ns[c], first, step, lb)
+            if ns_second is not None:
+                t += (h + (1 - h) * min(1.0, math.sqrt(max(0.0, f)))) * lookup_ns(ns_second[c], first, step, lb)
+            cost = t + ns_per_match * (h + (1 - h) * f) + work * (1 - h) * f
             cc = min(cc, cost)
         per.append(cc)
         if cc < best_cost:

@@ -135,6 +135,42 @@ def test_native_search_matches_oracle_loop():
     np.testing.assert_allclose(m.evaluate(q[ok], r["best"][ok], k), r["best_cost"][ok], rtol=1e-12)
 
 
+def test_native_search_with_second_half_matches_oracle_loop():
+    """The second half of a block: the native search and the oracle's loop
+    agree when the calibration carries it."""
+    m, bpk, fpr, ns = small_model()
+    ns2 = np.random.default_rng(9).uniform(0.0, 0.03, ns.shape)
+    m.ns_second = np.ascontiguousarray(ns2)
+    m.tables.ns_second = C.c_void_p(m.ns_second.ctypes.data)
+    q = CM.sample_queries(300, 6)
+    q["log2_n"] = np.random.default_rng(2).uniform(8, 22, len(q))
+    r = m.search(q, per_candidate=True, threads=2)
+    for i in range(len(q)):
+        b, bc, per = MO.search(bpk, fpr, 12.0, 2.0, ns, 0.003, 1 << 20, tuple(q[i])[:5], ns_second=ns2)
+        assert r["best"][i] == b
+        np.testing.assert_allclose(r["cand_cost"][i], per, rtol=1e-12)
+
+
+def test_loaded_filter_costs_more_at_few_bits_per_key():
+    """A filter with few bits per key has most of its bits set, so many
+    non-members pass the first half of a block and load the second: priced
+    on a zeroed filter (the first half only) such a candidate looks cheaper
+    than it is.  With the second half in the tables the low-bits/key cost
+    rises by (h + (1 - h) sqrt(f)) * second half, the high-bits/key one barely."""
+    m, bpk, fpr, ns = small_model()
+    q = CM.make_queries([16.0] * 2, [1.0] * 2, [0.0] * 2, [5.0] * 2, [0] * 2)
+    c = np.array([0, 0], dtype=np.int32)
+    k = np.array([0, len(bpk) - 1], dtype=np.uint32)   # fewest and most bits per key
+    zeroed = m.evaluate(q, c, k)
+    ns2 = np.full(ns.shape, 0.02)
+    m.ns_second = np.ascontiguousarray(ns2)
+    m.tables.ns_second = C.c_void_p(m.ns_second.ctypes.data)
+    loaded = m.evaluate(q, c, k)
+    want = np.sqrt(fpr[0, k]) * 0.02
+    np.testing.assert_allclose(loaded - zeroed, want, rtol=1e-12)
+    assert (loaded - zeroed)[0] > 5 * (loaded - zeroed)[1]
+
+
 def test_repair_moves_to_the_nearest_feasible_size():
     m, bpk, fpr, ns = small_model()
     q = CM.make_queries([16.0, 16.0], [fpr[2, 10], 1.0], [0.1, 0.1], [50.0, 50.0], [0, 1])
