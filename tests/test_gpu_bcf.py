@@ -233,3 +233,28 @@ def test_partitioned_build():
         del w
         torch.cuda.empty_cache()
     assert abs(fps[0] - fps[1]) <= 0.25 * fps[1] + 5 * np.sqrt(fps[1] + 1), fps
+
+
+def test_partitioned_build_with_overflowing_range():
+    """Blocked cuckoo keys skewed into one 8 MiB range overflow its segment of
+    the partition; those keys come from the exact spill list (a second insert
+    of a cuckoo key would take a second slot): every key placed once, no
+    false negatives, the GPU's probe of the table equal to the oracle's."""
+    m = 1 << 31                                   # 256 MiB, 64-byte blocks: 32 ranges of 2^17 blocks
+    o = O.BlockedCuckoo(m, 64, 16, 4)
+    f = F.bcf(m, 64, 16, 4)
+    c1 = 370248451                                # the blocked cuckoo's block hash constant
+    out, start = [], 0
+    while sum(len(x) for x in out) < 1 << 20:
+        k = keygen.build_keys(1 << 23, 81, start=start)
+        start += 1 << 23
+        out.append(k[((k.astype(np.uint64) * np.uint64(c1)) & np.uint64(0xFFFFFFFF)) < np.uint64(1 << 27)])
+    bk = np.concatenate(out)[: 1 << 20]          # all in range 0: a quarter of its slots
+    f.set_build_options(2)
+    w = f.alloc_filter_data()
+    assert f.batch_insert(w, dev_keys(bk))
+    f.set_build_options(0)
+    words = host64(w)
+    assert len(o.batch_contains(words, bk)) == len(bk)
+    pk = np.concatenate([bk[::7], keygen.build_keys(100000, 82, start=1 << 30)])
+    assert np.array_equal(gpu_probe(f, w, pk, 3), o.batch_contains(words, pk, 3))

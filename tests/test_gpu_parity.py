@@ -276,3 +276,42 @@ def test_partitioned_build_large_filter():
         assert len(ob.batch_contains(words, sample)) == len(sample)
         del auto, direct
         torch.cuda.empty_cache()
+
+
+def _keys_in_top_half(n, seed, mul):
+    """n distinct keys whose hash key * mul (mod 2^32) is below 2^31."""
+    out, start = [], 0
+    while sum(len(o) for o in out) < n:
+        k = keygen.build_keys(4 * n, seed, start=start)
+        start += 4 * n
+        out.append(k[((k.astype(np.uint64) * np.uint64(mul)) & np.uint64(0xFFFFFFFF)) < np.uint64(1 << 31)])
+    return np.concatenate(out)[:n]
+
+
+def test_partitioned_plan_with_overflowing_range():
+    """The partition gives every range a segment of its expected share plus
+    slack; keys skewed into one range overflow it, and the overflowing keys
+    are probed (inserted) straight from the key array.  A POW2 filter of two
+    8 MiB ranges; 95 % of the keys hash into the first: the partitioned probe
+    and the partitioned build still equal the oracle."""
+    m = 1 << 27                                   # 16 MiB: 2^18 64-byte blocks, ranges of 2^17
+    ob = O.Bloom(8, 8, 8, 1, 8, m)
+    f = F.bbf_64(m, 8, 8, 8)
+    c0 = 596572387                                # the block hash constant, hash_family.hpp
+    skew = _keys_in_top_half(1 << 20, 71, c0)     # block < 2^17: range 0
+    bk = np.concatenate([skew[: 950000], keygen.build_keys(50000, 72)])
+    rw = ob.alloc()
+    ob.insert(rw, bk)
+    f.set_build_options(2)
+    words = f.alloc_filter_data()
+    assert f.batch_insert(words, dev_keys(bk, pad=2))
+    f.set_build_options(0)
+    assert np.array_equal(words.cpu().numpy().view(np.uint64)[:len(rw)], rw)
+    pk = np.concatenate([skew[500000:], keygen.probe_keys(50000, 200001, 0.3, 72)[0]])
+    np.random.default_rng(3).shuffle(pk)
+    exp = ob.batch_contains(rw, pk, 5)
+    for variant in (0, 1):
+        f.set_probe_options(3, variant)
+        for pad in (0, 1):
+            assert np.array_equal(gpu_probe(f, words, pk, 5, pad), exp), (variant, pad)
+    f.set_probe_options(0, -1)
