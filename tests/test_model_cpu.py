@@ -193,6 +193,35 @@ def test_committed_calibration_data():
 
 
 @pytest.mark.skipif(not os.path.exists(DEFAULT_PATH), reason="no calibration data")
+def test_committed_calibration_prices_the_second_half():
+    """The committed GPU calibration times every layout on a zeroed and on a
+    half-filled filter.  Blocks that are tested in two halves (64-byte
+    sectorized) pay a second half that a zeroed filter never shows; one-word
+    blocks have none.  A sectorized filter at few bits per key (most bits
+    set, so many non-members pass the first half) is then priced well above
+    its zeroed-filter cost, one at many bits per key barely above it."""
+    cal = CalibrationData.load()
+    assert cal.ns_second is not None and cal.ns_second.shape == cal.ns_per_key.shape
+    assert (cal.ns_second >= 0).all() and np.isfinite(cal.ns_second).all()
+    names = [c.name for c in cal.candidates]
+    sect, one = names.index("bbf u64 w=8 s=8 z=1 k=8"), names.index("bbf u32 w=1 s=1 z=1 k=4")
+    l2 = (cal.log2_bytes >= 16) & (cal.log2_bytes <= 26)       # 64 KiB .. 64 MiB
+    assert cal.ns_second[sect, l2].mean() > 0.2 * cal.ns_per_key[sect, l2].mean()
+    assert cal.ns_second[one].max() < 0.1 * cal.ns_per_key[one].min()     # timing noise only
+    loaded = CM.CostModel(cal)
+    zeroed = CM.CostModel(CalibrationData(cal.candidates, cal.log2_bytes, cal.ns_per_key, cal.ns_per_match,
+                                          cal.meta))
+    # no downstream work: the cost is the probe time plus the match writes
+    q = CM.make_queries([20.0, 20.0], [1.0, 1.0], [0.0, 0.0], [0.0, 0.0], [0, 0])
+    k = loaded.bpk_index([4.0, 24.0]).astype(np.uint32)
+    c = np.array([sect, sect], dtype=np.int32)
+    lo, hi = loaded.evaluate(q, c, k), zeroed.evaluate(q, c, k)
+    probe0 = hi - cal.ns_per_match * loaded.fpr[sect, k]   # zeroed-filter probe time
+    assert lo[0] - hi[0] > 0.15 * probe0[0]       # 4 bits per key: the second half is paid often
+    assert lo[1] - hi[1] < 0.05 * probe0[1]       # 24 bits per key: rarely
+
+
+@pytest.mark.skipif(not os.path.exists(DEFAULT_PATH), reason="no calibration data")
 def test_skyline_and_search_on_committed_data():
     model = CM.CostModel(CalibrationData.load())
     q = CM.feasible_queries(model, 300, 4)
