@@ -129,18 +129,19 @@ size_t round256(uint64_t b) { return static_cast<size_t>(((b + 255) / 256) * 256
 uint32_t part_tiles(uint64_t n_phys) { return static_cast<uint32_t>((n_phys + kPartTile - 1) / kPartTile); }
 
 // Workspace: header | status words | match bitmask | [partitioned probe:
-// range counts | range totals | (key, position) pairs]
+// partition header (range fill counters) | per-tile overflow masks |
+// (key, position) pairs in one segment per range]
 struct WsLayout {
-  size_t bits_off, counts_off, totals_off, pairs_off, total_small, total;
+  size_t bits_off, part_off, tflags_off, pairs_off, total_small, total;
 };
 WsLayout ws_layout(uint64_t n_phys) {
   WsLayout l{};
   l.bits_off = sizeof(WsHeader) + status_bytes(n_phys);
-  l.counts_off = l.bits_off + round256(bits_words(n_phys) * 4);
-  l.total_small = l.counts_off;
-  l.totals_off = l.counts_off + round256(static_cast<uint64_t>(kMaxRanges) * part_tiles(n_phys) * 4);
-  l.pairs_off = l.totals_off + round256(kMaxRanges * 4);
-  l.total = l.pairs_off + round256(n_phys * 8 + 16);
+  l.part_off = l.bits_off + round256(bits_words(n_phys) * 4);
+  l.total_small = l.part_off;
+  l.tflags_off = l.part_off + kPartHeaderBytes;
+  l.pairs_off = l.tflags_off + round256(static_cast<uint64_t>(part_tiles(n_phys)) * 8);
+  l.total = l.pairs_off + round256(part_pair_capacity(n_phys) * 8 + 16);
   return l;
 }
 size_t workspace_bytes(uint64_t n_phys) { return ws_layout(n_phys).total; }
@@ -256,10 +257,23 @@ int probe_plan(const dtlg_filter* f, uint64_t n) {
 // 85.3 / 80.4 with 32 MiB ranges, 92.2 / 94.3 / 89.0 against 89.7 / 92.1 /
 // 90.5 with 8 MiB ranges; zoned u64 w=8 z=2 at 256 / 384 MiB 94.4 / 91.1
 // against 92.7 / 88.3.
+// A 32-register variant that spills (local memory per thread, from
+// cudaFuncGetAttributes) gives way to the 64-register one: -Xptxas -v shows
+// spills in the pair probe of 4 layouts with k = 16 and in the bitmask kernel
+// of 19 layouts, none of them among the layouts the rule above was measured on.
 int probe_variant(const dtlg_filter* f, int mode) {
   if (f->bits_variant >= 0 && f->bits_variant < kBitsVariants) return f->bits_variant;
-  if (mode == 3) return (f->d.kind == Kind::kBloom || f->d.kind == Kind::kZoned) ? 0 : 1;
-  return bitmask_band(f) ? 0 : 1;
+  int v;
+  if (mode == 3) {
+    v = (f->d.kind == Kind::kBloom || f->d.kind == Kind::kZoned) ? 0 : 1;
+  } else {
+    v = bitmask_band(f) ? 0 : 1;
+  }
+  if (v == 0) {
+    const occ_fn spill = mode == 3 ? f->pk->pairs_local_bytes[0] : f->pk->bits_local_bytes[0];
+    if (spill && spill() != 0) v = 1;
+  }
+  return v;
 }
 
 // Ranges of the partitioned probe and build: 2^L blocks each, about 8 MiB of
@@ -278,13 +292,15 @@ void partition_ranges(const dtlg_filter* f, uint32_t* range_log2, uint32_t* n_ra
   *n_ranges = static_cast<uint32_t>((nb + (1ull << L) - 1) >> L);
 }
 
-// Groups keys_al[pre, n_phys) by filter range: (key, logical position) pairs,
-// range by range, in the workspace's pair area (partitioned probe and build).
-// Grids of resident CTAs only: the tiles are strided over the grid, so a
-// second, partial wave would finish its share late (the scatter's 37 KiB of
-// shared memory allow 6 CTAs per SM, not 8).
+// Groups keys_al[pre, n_phys) by filter range: (key, logical position) pairs
+// in one segment per range, in the workspace's pair area (partitioned probe
+// and build).  The partition header must be zeroed before (it is, with the
+// match mask, by one memset).  One kernel, grids of resident CTAs only: the
+// tiles are strided over the grid, so a second, partial wave would finish its
+// share late.  spill: optional exact list of the pairs that did not fit.
 cudaError_t launch_partition(const dtlg_filter* f, const uint32_t* keys_al, uint64_t n_phys, uint32_t pre,
-                             char* wsb, const WsLayout& lay, int sms, cudaStream_t stream, PartArgs* out) {
+                             char* wsb, const WsLayout& lay, int sms, cudaStream_t stream, PartArgs* out,
+                             uint2* spill = nullptr) {
   PartArgs pa{};
   pa.keys_al = keys_al;
   pa.n_phys = n_phys;
@@ -293,23 +309,17 @@ cudaError_t launch_partition(const dtlg_filter* f, const uint32_t* keys_al, uint
   pa.block_mul = mul_const(f->xk ? 1 : 0);
   partition_ranges(f, &pa.range_log2, &pa.n_ranges);
   pa.n_tiles = part_tiles(n_phys);
-  pa.counts = reinterpret_cast<uint32_t*>(wsb + lay.counts_off);
-  pa.totals = reinterpret_cast<uint32_t*>(wsb + lay.totals_off);
+  part_segments(n_phys - pre, f->d.addr.block_cnt, pa.range_log2, pa.n_ranges, &pa.seg_cap, &pa.last_cap);
+  pa.hdr = reinterpret_cast<PartHeader*>(wsb + lay.part_off);
+  pa.tile_overflow = reinterpret_cast<unsigned long long*>(wsb + lay.tflags_off);
   pa.pairs = reinterpret_cast<uint2*>(wsb + lay.pairs_off);
-  static const int hist_occ = [] {
-    int o = 0;
-    return cudaOccupancyMaxActiveBlocksPerMultiprocessor(&o, part_hist_kernel, kPartThreads, 0) == cudaSuccess
-               ? std::max(1, o) : 1;
-  }();
+  pa.spill = spill;
   static const int scatter_occ = [] {
     int o = 0;
     return cudaOccupancyMaxActiveBlocksPerMultiprocessor(&o, part_scatter_kernel, kPartThreads, 0) == cudaSuccess
                ? std::max(1, o) : 1;
   }();
-  const int hgrid = static_cast<int>(std::min<uint64_t>(pa.n_tiles, static_cast<uint64_t>(sms) * hist_occ));
   const int sgrid = static_cast<int>(std::min<uint64_t>(pa.n_tiles, static_cast<uint64_t>(sms) * scatter_occ));
-  part_hist_kernel<<<hgrid, kPartThreads, 0, stream>>>(pa);
-  part_scan_kernel<<<pa.n_ranges, 1024, 0, stream>>>(pa);
   part_scatter_kernel<<<sgrid, kPartThreads, 0, stream>>>(pa);
   *out = pa;
   return cudaGetLastError();
@@ -401,14 +411,14 @@ dtlg_status launch_probe(const dtlg_filter* f, const uint64_t* words, const uint
       DTLG_CUDA(bfn(a, bits, r > 0 ? 1 : 0, bgrid, stream));
     }
   } else {
-    // partitioned probe: keys grouped by filter range, probed range by range
+    // partitioned probe: keys grouped by filter range, probed range by range;
+    // one memset zeroes the match mask and the partition header after it
     PartArgs pa{};
-    DTLG_CUDA(cudaMemsetAsync(bits, 0, bits_words(n_phys) * 4, stream));
+    DTLG_CUDA(cudaMemsetAsync(bits, 0, lay.part_off - lay.bits_off + kPartHeaderBytes, stream));
     DTLG_CUDA(launch_partition(f, a.keys_al, n_phys, pre, wsb, lay, ds->sms, stream, &pa));
     PairsArgs pr{};
     pr.probe = a;
-    pr.pairs = pa.pairs;
-    pr.n_pairs = n;
+    pr.part = pa;
     pr.bits = bits;
     pr.pre = pre;
     const int qgrid = static_cast<int>(static_cast<uint64_t>(ds->sms) * std::max(1, f->pk->pairs_blocks_per_sm[v]()));
@@ -664,14 +674,19 @@ dtlg_status dtlg_batch_insert(const dtlg_filter* f, uint64_t* words, const uint3
     static std::atomic<uint64_t> seed_ctr{0x13198A2E03707344ull};
     b.seed = seed_ctr.fetch_add(0x9E3779B97F4A7C15ull);
     if (block_build_plan(f, n) == 2) {
-      // keys grouped by L2-sized block range first, as for Bloom filters
+      // keys grouped by L2-sized block range first, as for Bloom filters; the
+      // pairs that overflow their segment go to an exact spill list after the
+      // workspace (a blocked cuckoo key must be inserted exactly once)
       const WsLayout lay = ws_layout(b.n_phys);
       void* ws = nullptr;
-      if (cudaMallocFromPoolAsync(&ws, lay.total, ds->pool, stream) == cudaSuccess) {
+      if (cudaMallocFromPoolAsync(&ws, lay.total + round256(b.n_phys * 8), ds->pool, stream) == cudaSuccess) {
         PartArgs pa{};
-        cudaError_t e =
-            launch_partition(f, b.keys_al, b.n_phys, pre, static_cast<char*>(ws), lay, ds->sms, stream, &pa);
-        if (e == cudaSuccess) e = f->xk->insert_pairs(b, pa.pairs, n, grid_for(n, ds->sms), stream);
+        char* wsb = static_cast<char*>(ws);
+        cudaError_t e = cudaMemsetAsync(wsb + lay.part_off, 0, kPartHeaderBytes, stream);
+        if (e == cudaSuccess)
+          e = launch_partition(f, b.keys_al, b.n_phys, pre, wsb, lay, ds->sms, stream, &pa,
+                               reinterpret_cast<uint2*>(wsb + lay.total));
+        if (e == cudaSuccess) e = f->xk->insert_pairs(b, pa, grid_for(n, ds->sms), stream);
         cudaFreeAsync(ws, stream);
         DTLG_CUDA(e);
         return DTLG_OK;
@@ -689,10 +704,12 @@ dtlg_status dtlg_batch_insert(const dtlg_filter* f, uint64_t* words, const uint3
     void* ws = nullptr;
     if (cudaMallocFromPoolAsync(&ws, lay.total, ds->pool, stream) == cudaSuccess) {
       PartArgs pa{};
-      cudaError_t e = launch_partition(f, keys - pre, n_phys, pre, static_cast<char*>(ws), lay, ds->sms, stream, &pa);
+      char* wsb = static_cast<char*>(ws);
+      cudaError_t e = cudaMemsetAsync(wsb + lay.part_off, 0, kPartHeaderBytes, stream);
+      if (e == cudaSuccess) e = launch_partition(f, keys - pre, n_phys, pre, wsb, lay, ds->sms, stream, &pa);
       if (e == cudaSuccess) {
         const uint64_t vec = (static_cast<uint64_t>(n) + 1) / 2;
-        e = f->bk->build_pairs(pa.pairs, n, words, f->d.addr, grid_for(vec, ds->sms), stream);
+        e = f->bk->build_pairs(pa, words, f->d.addr, grid_for(vec, ds->sms), stream);
       }
       cudaFreeAsync(ws, stream);
       DTLG_CUDA(e);
@@ -733,7 +750,8 @@ dtlg_status dtlg_set_l2_fetch_granularity(int bytes, int* in_effect) {
 int dtlg_probe_kernel_count(const dtlg_filter* f, uint32_t key_cnt) {
   if (!f || key_cnt == 0) return 0;
   const int mode = probe_plan(f, key_cnt);
-  return mode == 1 ? 1 : (mode == 2 ? static_cast<int>(probe_passes(f)) + 1 : (mode == 4 ? 2 : 5));
+  // plan 3: partition scatter, pair probe, overflow keys, compaction
+  return mode == 1 ? 1 : (mode == 2 ? static_cast<int>(probe_passes(f)) + 1 : (mode == 4 ? 2 : 4));
 }
 
 dtlg_status dtlg_set_probe_passes(dtlg_filter* f, int passes) {

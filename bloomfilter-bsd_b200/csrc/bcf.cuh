@@ -265,12 +265,16 @@ __global__ void __launch_bounds__(256) bcf_insert_kernel(const __grid_constant__
 // The same over range-grouped (key, position) pairs (probe3.cuh's
 // partition): consecutive keys hit the same L2-sized block range, so the
 // compare-and-swap steps of a filter far larger than L2 work on lines in L2.
+// A second insert of a key would take a second slot, so the keys whose run
+// overflowed its segment come from the partition's exact spill list.
 template <class Cfg>
 __global__ void __launch_bounds__(256) bcf_insert_pairs_kernel(const __grid_constant__ BcfBuildArgs a,
-                                                               const uint2* __restrict__ pairs, uint64_t n_pairs) {
-  for (uint64_t p = blockIdx.x * static_cast<uint64_t>(blockDim.x) + threadIdx.x; p < n_pairs;
+                                                               const __grid_constant__ PartArgs pa) {
+  for_each_pair(seg_chunks(pa), [&](uint32_t key, uint32_t pos) { bcf_insert_key<Cfg>(a, key, pos); });
+  const uint32_t n_spill = pa.hdr->spill_cnt;
+  for (uint64_t p = blockIdx.x * static_cast<uint64_t>(blockDim.x) + threadIdx.x; p < n_spill;
        p += static_cast<uint64_t>(gridDim.x) * blockDim.x) {
-    const uint2 x = __ldcs(pairs + p);
+    const uint2 x = pa.spill[p];
     bcf_insert_key<Cfg>(a, x.x, x.y);
   }
 }

@@ -11,6 +11,7 @@
 
 #include "common.cuh"
 #include "probe.cuh"
+#include "probe3.cuh"
 
 namespace dtlg {
 
@@ -68,6 +69,12 @@ __device__ __forceinline__ uint4 ld_weak_128(const void* p) {
   asm volatile("ld.global.v4.u32 {%0,%1,%2,%3}, [%4];" : "=r"(r.x), "=r"(r.y), "=r"(r.z), "=r"(r.w) : "l"(p));
   return r;
 }
+// 256 bits coherently, for a 32-byte aligned address: one L1 wavefront for a
+// 32-byte half block where two 128-bit loads take two.
+__device__ __forceinline__ void ld_weak_256(const void* p, unsigned long long& a, unsigned long long& b,
+                                            unsigned long long& c, unsigned long long& d) {
+  asm volatile("ld.global.v4.u64 {%0,%1,%2,%3}, [%4];" : "=l"(a), "=l"(b), "=l"(c), "=l"(d) : "l"(p));
+}
 __device__ __forceinline__ unsigned long long ld_weak_64(const void* p) {
   unsigned long long r;
   asm volatile("ld.global.u64 %0, [%1];" : "=l"(r) : "l"(p));
@@ -89,6 +96,15 @@ template <typename Word, int W, bool NC = true>
 __device__ __forceinline__ void load_block(const Word* base, Word (&v)[W], bool vec32 = false, bool l1na = false) {
   constexpr int kBytes = W * static_cast<int>(sizeof(Word));
   if constexpr (!NC) {
+    if constexpr (kBytes >= 32) {
+      if (vec32) {
+        unsigned long long* d = reinterpret_cast<unsigned long long*>(&v[0]);
+        const unsigned long long* p = reinterpret_cast<const unsigned long long*>(base);
+#pragma unroll
+        for (int i = 0; i < kBytes / 32; i++) ld_weak_256(p + 4 * i, d[4 * i], d[4 * i + 1], d[4 * i + 2], d[4 * i + 3]);
+        return;
+      }
+    }
     if constexpr (kBytes >= 16) {
 #pragma unroll
       for (int i = 0; i < kBytes / 16; i++) {
@@ -234,9 +250,9 @@ struct BloomOps {
         }
       } else {
         Word v[kH];
-        load_block<Word, kH, false>(base, v);
+        load_block<Word, kH, false>(base, v, vec32);
         if (!test_words<0, kH>(v, key)) return false;
-        load_block<Word, kH, false>(base + kH, v);
+        load_block<Word, kH, false>(base + kH, v, vec32);
         return test_words<kH, kW>(v, key);
       }
     }
@@ -326,18 +342,15 @@ __global__ void __launch_bounds__(256) bloom_build_kernel(const __grid_constant_
 
 // batch_insert of range-grouped (key, position) pairs (probe3.cuh's
 // partition): consecutive keys hit the same L2-sized block range, so the
-// atomic ORs of a filter far larger than L2 update lines that sit in L2.
+// atomic ORs of a filter far larger than L2 update lines that sit in L2.  Keys
+// whose run overflowed its segment are inserted from the key array (inserting
+// a key twice sets the same bits).
 template <class Cfg>
-__global__ void __launch_bounds__(256) bloom_build_pairs_kernel(const uint2* __restrict__ pairs, uint64_t n_pairs,
-                                                                void* filter, const Addr addr) {
-  const uint4* p4 = reinterpret_cast<const uint4*>(pairs);
-  const uint64_t n2 = (n_pairs + 1) >> 1;  // two pairs per 16-byte vector
-  for (uint64_t i = blockIdx.x * static_cast<uint64_t>(blockDim.x) + threadIdx.x; i < n2;
-       i += static_cast<uint64_t>(gridDim.x) * blockDim.x) {
-    const uint4 x = __ldcs(p4 + i);
-    BloomOps<Cfg>::insert(filter, x.x, addr);
-    if (2 * i + 1 < n_pairs) BloomOps<Cfg>::insert(filter, x.z, addr);
-  }
+__global__ void __launch_bounds__(256) bloom_build_pairs_kernel(const __grid_constant__ PartArgs pa, void* filter,
+                                                                const Addr addr) {
+  auto ins = [&](uint32_t key, uint32_t) { BloomOps<Cfg>::insert(filter, key, addr); };
+  for_each_pair(seg_chunks(pa), ins);
+  for_each_overflow_key(pa, ins);
 }
 
 #endif  // __CUDACC__

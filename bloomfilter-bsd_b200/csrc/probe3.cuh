@@ -8,15 +8,30 @@
 // in range order, so the filter is read from DRAM about once per pass instead
 // of once per key:
 //
-//   1. part_hist_kernel     per-tile key count of every range
-//   2. part_scan_kernel     per range: exclusive scan of the tile counts
-//   3. part_scatter_kernel  (key, position) pairs into their range's segment
-//   4. probe_pairs_kernel   probe each pair, set bit `position` of the
-//                           key-ordered match mask (zeroed beforehand)
-//   5. compact_kernel       (probe2.cuh) ascending positions from the mask
+//   1. part_scatter_kernel    one pass over the keys: each 4096-key tile is
+//                             sorted by range in shared memory, reserves room
+//                             for its run of every range with one atomic add
+//                             on that range's fill counter, and writes the
+//                             runs as (key, position) pairs into the range's
+//                             segment
+//   2. probe_pairs_kernel     probe the segments chunk by chunk in range
+//                             order; each match sets bit `position` of the
+//                             key-ordered match mask (zeroed beforehand)
+//   3. probe_overflow_kernel  the keys of runs that did not fit (see below)
+//   4. compact_kernel         (probe2.cuh) ascending positions from the mask
 //
-// Extra traffic against a direct probe: keys read twice (8 B), pairs written
-// and read (16 B), all sequential.
+// No counting pass: every segment has a fixed capacity, the range's expected
+// share of the keys (its block count over the filter's) plus 1/32 and one
+// tile, so the keys are read once.  For hashed keys the share is exceeded by
+// far less than that slack (at 2^28 keys the slack is ~60 standard deviations).
+// Whatever does not fit is still probed: the tile records, per range, that its
+// run overflowed, and the overflow kernel re-probes those keys straight from
+// the key array (a key probed twice sets the same mask bit twice).  Where a
+// second insert of a key is not harmless (blocked cuckoo builds) the
+// overflowing pairs are also written to an exact spill list.
+//
+// Extra traffic against a direct probe: pairs written and read (16 B/key),
+// all sequential.
 #pragma once
 
 #include <cstdint>
@@ -30,6 +45,22 @@ constexpr int kPartThreads = 256;
 constexpr int kPartKeysPerThread = 16;                  // 4 key vectors
 constexpr uint32_t kPartTile = kPartThreads * kPartKeysPerThread;  // 4096 keys
 constexpr int kMaxRanges = 64;
+constexpr uint32_t kPartChunk = 2048;                   // pairs per chunk of a segment
+constexpr uint32_t kPartHeaderBytes = 512;              // fill counters + overflow counters
+
+// Pairs the partition of n keys may need in all: the sum of the segment
+// capacities (share + share/32 + one tile, rounded up to a chunk, per range).
+__host__ __device__ constexpr uint64_t part_pair_capacity(uint64_t n) {
+  return n + n / 32 + static_cast<uint64_t>(kMaxRanges) * (kPartTile + kPartChunk);
+}
+
+// Header of the partition's workspace (zeroed before the scatter).
+struct PartHeader {
+  unsigned int fill[kMaxRanges];     // pairs requested per range (may exceed the capacity)
+  unsigned int overflow_tiles;       // tiles with at least one overflowing run
+  unsigned int spill_cnt;            // pairs in the spill list
+};
+static_assert(sizeof(PartHeader) <= kPartHeaderBytes, "partition header");
 
 struct PartArgs {
   const uint32_t* keys_al;  // 16-byte aligned key base (see ProbeArgs)
@@ -39,11 +70,28 @@ struct PartArgs {
   uint32_t range_log2;      // a range is 2^range_log2 consecutive blocks
   uint32_t n_ranges;
   uint32_t n_tiles;
-  uint32_t* counts;         // [n_ranges][n_tiles]: counts, then exclusive prefixes
-  uint32_t* totals;         // [n_ranges]
-  uint2* pairs;             // (key, logical position), grouped by range
   uint32_t block_mul;       // the family constant of the block hash (C[0]; C[1]: blocked cuckoo)
+  uint64_t seg_cap;         // capacity of every segment but the last (multiple of kPartChunk)
+  uint64_t last_cap;        // capacity of the last segment (multiple of kPartChunk)
+  uint2* pairs;             // (key, logical position); segment r starts at r * seg_cap
+  PartHeader* hdr;
+  unsigned long long* tile_overflow;  // [n_tiles]: bit r = the tile's run of range r overflowed
+  uint2* spill;             // optional: every overflowing pair (capacity n_phys)
 };
+
+// Host-side sizing of the segments for n keys over `blocks` blocks in ranges
+// of 2^range_log2 blocks.
+inline void part_segments(uint64_t n, uint64_t blocks, uint32_t range_log2, uint32_t n_ranges, uint64_t* seg_cap,
+                          uint64_t* last_cap) {
+  auto cap = [&](uint64_t range_blocks) {
+    const uint64_t share = (n * range_blocks + blocks - 1) / blocks;
+    const uint64_t c = share + share / 32 + kPartTile;
+    return (c + kPartChunk - 1) / kPartChunk * kPartChunk;
+  };
+  const uint64_t full = 1ull << range_log2;
+  *seg_cap = cap(full < blocks ? full : blocks);
+  *last_cap = cap(blocks - static_cast<uint64_t>(n_ranges - 1) * full);
+}
 
 #ifdef __CUDACC__
 
@@ -51,185 +99,206 @@ __device__ __forceinline__ uint32_t key_range(uint32_t key, const PartArgs& a) {
   return block_index(key * a.block_mul, a.addr) >> a.range_log2;
 }
 
-static __global__ void __launch_bounds__(kPartThreads) part_hist_kernel(const __grid_constant__ PartArgs a) {
-  __shared__ uint32_t hist[kMaxRanges];
-  const uint4* keys4 = reinterpret_cast<const uint4*>(a.keys_al);
-  for (uint32_t tile = blockIdx.x; tile < a.n_tiles; tile += gridDim.x) {
-    for (uint32_t r = threadIdx.x; r < a.n_ranges; r += blockDim.x) hist[r] = 0;
-    __syncthreads();
-    const uint64_t v0 = static_cast<uint64_t>(tile) * (kPartTile / 4);
-#pragma unroll
-    for (int i = 0; i < kPartKeysPerThread / 4; i++) {
-      const uint64_t v = v0 + static_cast<uint64_t>(i) * kPartThreads + threadIdx.x;
-      const uint64_t p0 = v * 4;
-      if (p0 >= a.n_phys) continue;
-      const uint4 kv = __ldcs(keys4 + v);
-      const uint32_t k[4] = {kv.x, kv.y, kv.z, kv.w};
-#pragma unroll
-      for (int q = 0; q < 4; q++)
-        if (p0 + q >= a.pre && p0 + q < a.n_phys) atomicAdd(&hist[key_range(k[q], a)], 1u);
-    }
-    __syncthreads();
-    for (uint32_t r = threadIdx.x; r < a.n_ranges; r += blockDim.x)
-      a.counts[static_cast<uint64_t>(r) * a.n_tiles + tile] = hist[r];
-    __syncthreads();
-  }
-}
-
-// One CTA per range: exclusive scan of that range's tile counts.
-static __global__ void __launch_bounds__(1024) part_scan_kernel(const __grid_constant__ PartArgs a) {
-  __shared__ uint32_t s_warp[32];
-  __shared__ uint32_t s_carry;
-  const uint32_t r = blockIdx.x;
-  uint32_t* c = a.counts + static_cast<uint64_t>(r) * a.n_tiles;
-  const uint32_t lane = threadIdx.x & 31u, warp = threadIdx.x >> 5;
-  if (threadIdx.x == 0) s_carry = 0;
-  __syncthreads();
-  for (uint32_t base = 0; base < a.n_tiles; base += blockDim.x) {
-    const uint32_t i = base + threadIdx.x;
-    const uint32_t v = i < a.n_tiles ? c[i] : 0u;
-    uint32_t incl = v;
-#pragma unroll
-    for (int d = 1; d < 32; d <<= 1) {
-      const uint32_t t = __shfl_up_sync(0xffffffffu, incl, d);
-      if (lane >= static_cast<uint32_t>(d)) incl += t;
-    }
-    if (lane == 31) s_warp[warp] = incl;
-    __syncthreads();
-    if (warp == 0) {
-      const uint32_t wv = s_warp[lane];
-      uint32_t wi = wv;
-#pragma unroll
-      for (int d = 1; d < 32; d <<= 1) {
-        const uint32_t t = __shfl_up_sync(0xffffffffu, wi, d);
-        if (lane >= static_cast<uint32_t>(d)) wi += t;
-      }
-      s_warp[lane] = wi - wv;
-    }
-    __syncthreads();
-    const uint32_t carry = s_carry;
-    if (i < a.n_tiles) c[i] = carry + s_warp[warp] + incl - v;
-    __syncthreads();
-    if (threadIdx.x == blockDim.x - 1) s_carry = carry + s_warp[warp] + incl;
-    __syncthreads();
-  }
-  if (threadIdx.x == 0) a.totals[r] = s_carry;
-}
-
-// Each tile is sorted by range in shared memory first, then every range's run
-// is written to its segment with consecutive addresses (coalesced stores).
-static __global__ void __launch_bounds__(kPartThreads) part_scatter_kernel(const __grid_constant__ PartArgs a) {
-  __shared__ uint2 s_pairs[kPartTile];
-  __shared__ unsigned char s_range[kPartTile];
+// One pass: per tile, count the keys of every range, reserve the tile's run of
+// each range in its segment (one global atomic per tile and range), sort the
+// tile by range in shared memory and write every run with consecutive
+// addresses.  Shared memory holds the sorted keys and their 12-bit tile
+// positions (24 KiB), so eight CTAs fit on an SM.
+static __global__ void __launch_bounds__(kPartThreads, 8) part_scatter_kernel(const __grid_constant__ PartArgs a) {
+  __shared__ uint32_t s_keys[kPartTile];
+  __shared__ uint16_t s_idx[kPartTile];
+  __shared__ uint32_t s_cur[kMaxRanges];    // counts, then the placement cursor
   __shared__ uint32_t s_lbase[kMaxRanges];  // tile-local start of each range's run
-  __shared__ uint32_t s_lcur[kMaxRanges];
-  __shared__ uint32_t s_gbase[kMaxRanges];  // global start of this tile's part of the range
+  __shared__ uint32_t s_gbase[kMaxRanges];  // the run's first slot in its segment
   __shared__ uint32_t s_valid;
+  __shared__ unsigned long long s_over;
   const uint4* keys4 = reinterpret_cast<const uint4*>(a.keys_al);
   const uint32_t lane = threadIdx.x & 31u;
   for (uint32_t tile = blockIdx.x; tile < a.n_tiles; tile += gridDim.x) {
-    if (threadIdx.x < 32) {
-      // this tile's count per range (difference of the scanned prefixes) and
-      // their exclusive scan; two ranges per lane
-      uint32_t cnt[2], gb[2];
-      uint32_t range_base = 0, sum_before = 0;
-      for (int h = 0; h < 2; h++) {
-        const uint32_t r = threadIdx.x * 2 + h;
-        cnt[h] = 0;
-        gb[h] = 0;
-        if (r < a.n_ranges) {
-          const uint32_t* c = a.counts + static_cast<uint64_t>(r) * a.n_tiles;
-          const uint32_t next = tile + 1 < a.n_tiles ? c[tile + 1] : a.totals[r];
-          cnt[h] = next - c[tile];
-          gb[h] = c[tile];
-        }
-      }
-      // range bases (exclusive scan of the totals) and tile-local bases
-      uint32_t t0 = (threadIdx.x * 2 < a.n_ranges) ? a.totals[threadIdx.x * 2] : 0u;
-      uint32_t t1 = (threadIdx.x * 2 + 1 < a.n_ranges) ? a.totals[threadIdx.x * 2 + 1] : 0u;
-      uint32_t pair_tot = t0 + t1, incl = pair_tot;
-      uint32_t pair_cnt = cnt[0] + cnt[1], cincl = pair_cnt;
-#pragma unroll
-      for (int d = 1; d < 32; d <<= 1) {
-        const uint32_t x = __shfl_up_sync(0xffffffffu, incl, d);
-        const uint32_t y = __shfl_up_sync(0xffffffffu, cincl, d);
-        if (lane >= static_cast<uint32_t>(d)) {
-          incl += x;
-          cincl += y;
-        }
-      }
-      range_base = incl - pair_tot;
-      sum_before = cincl - pair_cnt;
-      for (int h = 0; h < 2; h++) {
-        const uint32_t r = threadIdx.x * 2 + h;
-        if (r < kMaxRanges) {
-          s_gbase[r] = range_base + (h ? t0 : 0u) + gb[h];
-          s_lbase[r] = sum_before + (h ? cnt[0] : 0u);
-          s_lcur[r] = s_lbase[r];
-        }
-      }
-      if (threadIdx.x == 31) s_valid = cincl;
-    }
+    if (threadIdx.x < kMaxRanges) s_cur[threadIdx.x] = 0;
+    if (threadIdx.x == 0) s_over = 0;
     __syncthreads();
     const uint64_t v0 = static_cast<uint64_t>(tile) * (kPartTile / 4);
+    uint4 kv[kPartKeysPerThread / 4];
 #pragma unroll
     for (int i = 0; i < kPartKeysPerThread / 4; i++) {
       const uint64_t v = v0 + static_cast<uint64_t>(i) * kPartThreads + threadIdx.x;
-      const uint64_t p0 = v * 4;
-      uint4 kv = make_uint4(0, 0, 0, 0);
-      if (p0 < a.n_phys) kv = __ldcs(keys4 + v);
-      const uint32_t k[4] = {kv.x, kv.y, kv.z, kv.w};
+      kv[i] = v * 4 < a.n_phys ? __ldcs(keys4 + v) : make_uint4(0, 0, 0, 0);
+    }
+#pragma unroll
+    for (int i = 0; i < kPartKeysPerThread / 4; i++) {
+      const uint64_t p0 = (v0 + static_cast<uint64_t>(i) * kPartThreads + threadIdx.x) * 4;
+      const uint32_t k[4] = {kv[i].x, kv[i].y, kv[i].z, kv[i].w};
+#pragma unroll
+      for (int q = 0; q < 4; q++)
+        if (p0 + q >= a.pre && p0 + q < a.n_phys) atomicAdd(&s_cur[key_range(k[q], a)], 1u);
+    }
+    __syncthreads();
+    if (threadIdx.x < 32) {
+      // tile-local run starts (exclusive scan, two ranges per lane) and the
+      // runs' slots in their segments
+      const uint32_t r0 = lane * 2, r1 = lane * 2 + 1;
+      const uint32_t c0 = s_cur[r0], c1 = s_cur[r1];
+      const uint32_t pair = c0 + c1;
+      uint32_t incl = pair;
+#pragma unroll
+      for (int d = 1; d < 32; d <<= 1) {
+        const uint32_t x = __shfl_up_sync(0xffffffffu, incl, d);
+        if (lane >= static_cast<uint32_t>(d)) incl += x;
+      }
+      const uint32_t b0 = incl - pair;
+      s_lbase[r0] = b0;
+      s_lbase[r1] = b0 + c0;
+      s_cur[r0] = b0;
+      s_cur[r1] = b0 + c0;
+      s_gbase[r0] = c0 ? atomicAdd(&a.hdr->fill[r0], c0) : 0u;
+      s_gbase[r1] = c1 ? atomicAdd(&a.hdr->fill[r1], c1) : 0u;
+      if (lane == 31) s_valid = incl;
+    }
+    __syncthreads();
+#pragma unroll
+    for (int i = 0; i < kPartKeysPerThread / 4; i++) {
+      const uint64_t p0 = (v0 + static_cast<uint64_t>(i) * kPartThreads + threadIdx.x) * 4;
+      const uint32_t k[4] = {kv[i].x, kv[i].y, kv[i].z, kv[i].w};
 #pragma unroll
       for (int q = 0; q < 4; q++) {
-        const uint64_t p = p0 + q;
-        const bool valid = p >= a.pre && p < a.n_phys;
-        if (valid) {
-          const uint32_t r = key_range(k[q], a);
-          const uint32_t slot = atomicAdd(&s_lcur[r], 1u);
-          s_pairs[slot] = make_uint2(k[q], static_cast<uint32_t>(p - a.pre));
-          s_range[slot] = static_cast<unsigned char>(r);
+        if (p0 + q >= a.pre && p0 + q < a.n_phys) {
+          const uint32_t slot = atomicAdd(&s_cur[key_range(k[q], a)], 1u);
+          s_keys[slot] = k[q];
+          s_idx[slot] = static_cast<uint16_t>((i * kPartThreads + threadIdx.x) * 4 + q);
         }
       }
     }
     __syncthreads();
     const uint32_t nv = s_valid;
+    const uint64_t tile_pos = static_cast<uint64_t>(tile) * kPartTile;  // physical index of the tile's key 0
     for (uint32_t sl = threadIdx.x; sl < nv; sl += blockDim.x) {
-      const uint2 pr = s_pairs[sl];
-      const uint32_t r = s_range[sl];
-      __stcs(a.pairs + s_gbase[r] + (sl - s_lbase[r]), pr);
+      const uint32_t key = s_keys[sl];
+      const uint32_t r = key_range(key, a);
+      const uint64_t g = static_cast<uint64_t>(s_gbase[r]) + (sl - s_lbase[r]);
+      const uint64_t cap = r + 1 < a.n_ranges ? a.seg_cap : a.last_cap;
+      const uint2 pr = make_uint2(key, static_cast<uint32_t>(tile_pos + s_idx[sl] - a.pre));
+      if (g < cap) {
+        __stcs(a.pairs + static_cast<uint64_t>(r) * a.seg_cap + g, pr);
+      } else {
+        atomicOr(&s_over, 1ull << r);
+        if (a.spill) a.spill[atomicAdd(&a.hdr->spill_cnt, 1u)] = pr;
+      }
     }
     __syncthreads();
+    if (threadIdx.x == 0) {
+      a.tile_overflow[tile] = s_over;
+      if (s_over) atomicAdd(&a.hdr->overflow_tiles, 1u);
+    }
+  }
+}
+
+// The segments as a list of chunks of kPartChunk pairs, in range order.
+struct SegChunks {
+  const uint2* pairs;
+  uint64_t seg_cap, last_cap;
+  uint32_t n_ranges;
+  uint32_t chunks_per_seg;  // seg_cap / kPartChunk
+  uint32_t n_chunks;        // (n_ranges - 1) * chunks_per_seg + last_cap / kPartChunk
+  const PartHeader* hdr;
+};
+
+__host__ __device__ inline SegChunks seg_chunks(const PartArgs& pa) {
+  SegChunks s{};
+  s.pairs = pa.pairs;
+  s.seg_cap = pa.seg_cap;
+  s.last_cap = pa.last_cap;
+  s.n_ranges = pa.n_ranges;
+  s.chunks_per_seg = static_cast<uint32_t>(pa.seg_cap / kPartChunk);
+  s.n_chunks = (pa.n_ranges - 1) * s.chunks_per_seg + static_cast<uint32_t>(pa.last_cap / kPartChunk);
+  s.hdr = pa.hdr;
+  return s;
+}
+
+// Pairs of chunk c: first pair and count (0 .. kPartChunk).
+__device__ __forceinline__ uint32_t chunk_pairs(const SegChunks& s, uint32_t c, uint64_t* first) {
+  uint32_t r = c / s.chunks_per_seg;
+  if (r >= s.n_ranges) r = s.n_ranges - 1;
+  const uint64_t j0 = static_cast<uint64_t>(c - r * s.chunks_per_seg) * kPartChunk;
+  const uint64_t cap = r + 1 < s.n_ranges ? s.seg_cap : s.last_cap;
+  const uint64_t fill = s.hdr->fill[r];
+  const uint64_t filled = fill < cap ? fill : cap;
+  *first = static_cast<uint64_t>(r) * s.seg_cap + j0;
+  if (filled <= j0) return 0u;
+  return filled - j0 < kPartChunk ? static_cast<uint32_t>(filled - j0) : kPartChunk;
+}
+
+// Runs fn(key, position) over every pair of the segments: each CTA takes
+// whole chunks, the grid sweeping them in range order, so the CTAs in flight
+// work on one or two ranges at a time.  One 8-byte pair per thread and step
+// (two per 16-byte load needed more registers than the 32-register pair
+// probe has).
+template <class Fn>
+__device__ __forceinline__ void for_each_pair(const SegChunks& s, Fn fn) {
+  for (uint32_t c = blockIdx.x; c < s.n_chunks; c += gridDim.x) {
+    uint64_t first = 0;
+    const uint32_t cnt = chunk_pairs(s, c, &first);
+    const uint2* p = s.pairs + first;
+    for (uint32_t j = threadIdx.x; j < cnt; j += blockDim.x) {
+      const uint2 x = __ldcs(p + j);
+      fn(x.x, x.y);
+    }
+  }
+}
+
+// Runs fn(key, logical position) over the keys of every tile whose run of the
+// key's range overflowed its segment (all keys of that range in that tile,
+// the ones that did fit included); nothing when no tile overflowed.
+template <class Fn>
+__device__ __forceinline__ void for_each_overflow_key(const PartArgs& pa, Fn fn) {
+  if (pa.hdr->overflow_tiles == 0) return;
+  const uint4* keys4 = reinterpret_cast<const uint4*>(pa.keys_al);
+  for (uint32_t tile = blockIdx.x; tile < pa.n_tiles; tile += gridDim.x) {
+    const unsigned long long mask = pa.tile_overflow[tile];
+    if (mask == 0) continue;
+    const uint64_t v0 = static_cast<uint64_t>(tile) * (kPartTile / 4);
+    for (uint32_t i = threadIdx.x; i < kPartTile / 4; i += blockDim.x) {
+      const uint64_t v = v0 + i;
+      if (v * 4 >= pa.n_phys) break;
+      const uint4 kv = keys4[v];
+      const uint32_t k[4] = {kv.x, kv.y, kv.z, kv.w};
+#pragma unroll
+      for (int q = 0; q < 4; q++) {
+        const uint64_t p = v * 4 + q;
+        if (p >= pa.pre && p < pa.n_phys && ((mask >> key_range(k[q], pa)) & 1ull))
+          fn(k[q], static_cast<uint32_t>(p - pa.pre));
+      }
+    }
   }
 }
 
 struct PairsArgs {
   ProbeArgs probe;          // filter + addressing (keys fields unused)
-  const uint2* pairs;
-  uint64_t n_pairs;
+  PartArgs part;            // the partition the pairs came from
   uint32_t* bits;           // key-ordered match mask (bit = physical key index), zeroed
   uint32_t pre;             // physical index of the first key
 };
 
+template <class Ops>
+__device__ __forceinline__ void probe_pair(const PairsArgs& a, uint32_t key, uint32_t pos) {
+  if (Ops::contains(a.probe, key)) {
+    const uint64_t b = static_cast<uint64_t>(pos) + a.pre;
+    atomicOr(a.bits + (b >> 5), 1u << (b & 31u));
+  }
+}
+
 // Probes the pairs in range order; each match sets one bit of the mask.
 template <class Ops, int MINB>
 __global__ void __launch_bounds__(256, MINB) probe_pairs_kernel(const __grid_constant__ PairsArgs a) {
-  const uint4* p4 = reinterpret_cast<const uint4*>(a.pairs);
-  const uint64_t n2 = (a.n_pairs + 1) >> 1;  // two pairs per 16-byte vector
-  const uint64_t stride = static_cast<uint64_t>(gridDim.x) * blockDim.x;
-  for (uint64_t i = static_cast<uint64_t>(blockIdx.x) * blockDim.x + threadIdx.x; i < n2; i += stride) {
-    const uint4 x = __ldcs(p4 + i);
-    const bool has2 = 2 * i + 1 < a.n_pairs;
-    const bool m0 = Ops::contains(a.probe, x.x);
-    const bool m1 = has2 && Ops::contains(a.probe, x.z);
-    if (m0) {
-      const uint64_t b = static_cast<uint64_t>(x.y) + a.pre;
-      atomicOr(a.bits + (b >> 5), 1u << (b & 31u));
-    }
-    if (m1) {
-      const uint64_t b = static_cast<uint64_t>(x.w) + a.pre;
-      atomicOr(a.bits + (b >> 5), 1u << (b & 31u));
-    }
-  }
+  for_each_pair(seg_chunks(a.part), [&](uint32_t key, uint32_t pos) { probe_pair<Ops>(a, key, pos); });
+}
+
+// The keys of overflowing runs, after probe_pairs_kernel: a kernel of its
+// own, so that the pair kernel's register budget holds only its loop.  When
+// no segment filled up (the rule for hashed keys) every CTA returns at once.
+template <class Ops>
+__global__ void __launch_bounds__(256) probe_overflow_kernel(const __grid_constant__ PairsArgs a) {
+  for_each_overflow_key(a.part, [&](uint32_t key, uint32_t pos) { probe_pair<Ops>(a, key, pos); });
 }
 
 #endif  // __CUDACC__

@@ -39,6 +39,8 @@ struct ProbeKernels {
   pairs_fn probe_pairs[kBitsVariants];          // plan 3: partitioned (null: not offered)
   occ_fn pairs_blocks_per_sm[kBitsVariants];
   smem_fn probe_smem;                           // plan 4: filter in shared memory (null: not offered)
+  occ_fn bits_local_bytes[kBitsVariants];       // register spills per thread of each variant
+  occ_fn pairs_local_bytes[kBitsVariants];
 };
 
 struct BloomKernels {
@@ -46,8 +48,7 @@ struct BloomKernels {
   ProbeKernels pk;
   build_fn build;
   // build from range-grouped (key, position) pairs
-  cudaError_t (*build_pairs)(const uint2* pairs, uint64_t n_pairs, void* filter, const Addr& addr, int grid,
-                             cudaStream_t);
+  cudaError_t (*build_pairs)(const PartArgs& part, void* filter, const Addr& addr, int grid, cudaStream_t);
 };
 
 struct CuckooKernels {
@@ -66,7 +67,7 @@ struct BcfKernels {
   ProbeKernels pk;
   cudaError_t (*insert)(const BcfBuildArgs&, int grid, cudaStream_t);
   // insert from range-grouped (key, position) pairs
-  cudaError_t (*insert_pairs)(const BcfBuildArgs&, const uint2* pairs, uint64_t n_pairs, int grid, cudaStream_t);
+  cudaError_t (*insert_pairs)(const BcfBuildArgs&, const PartArgs& part, int grid, cudaStream_t);
 };
 
 struct ClassicKernels {
@@ -100,18 +101,36 @@ struct BitsLaunch {
     cudaOccupancyMaxActiveBlocksPerMultiprocessor(&n, probe_bits_kernel<Ops, MINB>, 256, 0);
     return n;
   }
+  static int local_bytes() {
+    static const int v = local_bytes_of(probe_bits_kernel<Ops, MINB>);
+    return v;
+  }
 };
+
+// Local memory of a kernel per thread (register spills; none of these
+// kernels has a stack otherwise), -1 if the query fails.
+template <class K>
+int local_bytes_of(K kernel) {
+  cudaFuncAttributes at{};
+  return cudaFuncGetAttributes(&at, kernel) == cudaSuccess ? static_cast<int>(at.localSizeBytes) : -1;
+}
 
 template <class Ops, int MINB>
 struct PairsLaunch {
+  // the pair probe, then the keys of overflowing runs (returns at once when none)
   static cudaError_t run(const PairsArgs& a, int grid, cudaStream_t s) {
     probe_pairs_kernel<Ops, MINB><<<grid, 256, 0, s>>>(a);
+    probe_overflow_kernel<Ops><<<grid, 256, 0, s>>>(a);
     return cudaGetLastError();
   }
   static int occupancy() {
     int n = 0;
     cudaOccupancyMaxActiveBlocksPerMultiprocessor(&n, probe_pairs_kernel<Ops, MINB>, 256, 0);
     return n;
+  }
+  static int local_bytes() {
+    static const int v = local_bytes_of(probe_pairs_kernel<Ops, MINB>);
+    return v;
   }
 };
 
@@ -134,9 +153,8 @@ struct BloomLaunch {
     bloom_build_kernel<Cfg><<<grid, 256, 0, s>>>(a);
     return cudaGetLastError();
   }
-  static cudaError_t build_pairs(const uint2* pairs, uint64_t n_pairs, void* filter, const Addr& addr, int grid,
-                                 cudaStream_t s) {
-    bloom_build_pairs_kernel<Cfg><<<grid, 256, 0, s>>>(pairs, n_pairs, filter, addr);
+  static cudaError_t build_pairs(const PartArgs& part, void* filter, const Addr& addr, int grid, cudaStream_t s) {
+    bloom_build_pairs_kernel<Cfg><<<grid, 256, 0, s>>>(part, filter, addr);
     return cudaGetLastError();
   }
 };
@@ -177,13 +195,16 @@ ProbeKernels probe_entry() {
   using P8 = PairsLaunch<Ops, 8>;
   using P4 = PairsLaunch<Ops, 4>;
   ProbeKernels k{&F::run, &F::occupancy, {&B8::run, &B4::run}, {&B8::occupancy, &B4::occupancy},
-                 {nullptr, nullptr}, {nullptr, nullptr}, nullptr};
+                 {nullptr, nullptr}, {nullptr, nullptr}, nullptr, {&B8::local_bytes, &B4::local_bytes},
+                 {nullptr, nullptr}};
   if constexpr (Smem) k.probe_smem = &SmemLaunch<Ops>::run;
   if constexpr (Pairs) {
     k.probe_pairs[0] = &P8::run;
     k.probe_pairs[1] = &P4::run;
     k.pairs_blocks_per_sm[0] = &P8::occupancy;
     k.pairs_blocks_per_sm[1] = &P4::occupancy;
+    k.pairs_local_bytes[0] = &P8::local_bytes;
+    k.pairs_local_bytes[1] = &P4::local_bytes;
   }
   return k;
 }
@@ -228,9 +249,8 @@ struct BcfLaunch {
     bcf_insert_kernel<BcfCfg<T, A>><<<grid, 256, 0, s>>>(a);
     return cudaGetLastError();
   }
-  static cudaError_t insert_pairs(const BcfBuildArgs& a, const uint2* pairs, uint64_t n_pairs, int grid,
-                                  cudaStream_t s) {
-    bcf_insert_pairs_kernel<BcfCfg<T, A>><<<grid, 256, 0, s>>>(a, pairs, n_pairs);
+  static cudaError_t insert_pairs(const BcfBuildArgs& a, const PartArgs& part, int grid, cudaStream_t s) {
+    bcf_insert_pairs_kernel<BcfCfg<T, A>><<<grid, 256, 0, s>>>(a, part);
     return cudaGetLastError();
   }
 };

@@ -123,12 +123,13 @@ def test_automatic_probe_plan(cfg, mib, plan):
     """The planner's choice for 2^28 probes (host logic only): the bitmask plan
     in block-range passes up to 160 MiB and, beyond, in the band of layouts it
     was measured faster for (s < w, one-word blocks, zoned u32); the
-    partitioned plan (5 kernels) otherwise.  Fewer than 2^20 keys: the fused
+    partitioned plan (4 kernels: scatter, pair probe,
+    overflow keys, compaction) otherwise.  Fewer than 2^20 keys: the fused
     single-kernel plan."""
     wb, w, s, z, k = cfg
     f = F.construct(F.blocked_bloomfilter_config(k=k, word_size=wb, word_cnt_per_block=w, sector_cnt=s,
                                                  zone_cnt=z), mib << 23)
     L = _lib.lib()
     kernels = L.dtlg_probe_kernel_count(f._h, 1 << 28)
-    assert (kernels == 5) == (plan == 3), (cfg, mib, kernels)
+    assert (kernels == 4) == (plan == 3), (cfg, mib, kernels)
     assert L.dtlg_probe_kernel_count(f._h, (1 << 20) - 1) == 1
