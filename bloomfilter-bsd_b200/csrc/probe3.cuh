@@ -103,7 +103,8 @@ __device__ __forceinline__ uint32_t key_range(uint32_t key, const PartArgs& a) {
 // each range in its segment (one global atomic per tile and range), sort the
 // tile by range in shared memory and write every run with consecutive
 // addresses.  Shared memory holds the sorted keys and their 12-bit tile
-// positions (24 KiB), so eight CTAs fit on an SM.
+// positions (24 KiB), so eight CTAs fit on an SM.  Inside a tile all index
+// arithmetic is 32-bit.
 static __global__ void __launch_bounds__(kPartThreads, 8) part_scatter_kernel(const __grid_constant__ PartArgs a) {
   __shared__ uint32_t s_keys[kPartTile];
   __shared__ uint16_t s_idx[kPartTile];
@@ -118,20 +119,26 @@ static __global__ void __launch_bounds__(kPartThreads, 8) part_scatter_kernel(co
     if (threadIdx.x < kMaxRanges) s_cur[threadIdx.x] = 0;
     if (threadIdx.x == 0) s_over = 0;
     __syncthreads();
-    const uint64_t v0 = static_cast<uint64_t>(tile) * (kPartTile / 4);
+    const uint64_t tile_pos = static_cast<uint64_t>(tile) * kPartTile;  // physical index of the tile's key 0
+    // valid keys of this tile: tile-local indexes [lo, hi)
+    const uint32_t lo = tile_pos < a.pre ? static_cast<uint32_t>(a.pre - tile_pos) : 0u;
+    const uint32_t hi = a.n_phys - tile_pos < kPartTile ? static_cast<uint32_t>(a.n_phys - tile_pos) : kPartTile;
+    const uint4* t4 = keys4 + tile_pos / 4;
+    // the keys are read twice: for the counts and, from L2, for the placement
+    // (holding them across the scan would not fit 32 registers)
     uint4 kv[kPartKeysPerThread / 4];
 #pragma unroll
     for (int i = 0; i < kPartKeysPerThread / 4; i++) {
-      const uint64_t v = v0 + static_cast<uint64_t>(i) * kPartThreads + threadIdx.x;
-      kv[i] = v * 4 < a.n_phys ? __ldcs(keys4 + v) : make_uint4(0, 0, 0, 0);
+      const uint32_t li = (i * kPartThreads + threadIdx.x) * 4;
+      kv[i] = li < hi ? __ldcg(t4 + li / 4) : make_uint4(0, 0, 0, 0);
     }
 #pragma unroll
     for (int i = 0; i < kPartKeysPerThread / 4; i++) {
-      const uint64_t p0 = (v0 + static_cast<uint64_t>(i) * kPartThreads + threadIdx.x) * 4;
+      const uint32_t li = (i * kPartThreads + threadIdx.x) * 4;
       const uint32_t k[4] = {kv[i].x, kv[i].y, kv[i].z, kv[i].w};
 #pragma unroll
       for (int q = 0; q < 4; q++)
-        if (p0 + q >= a.pre && p0 + q < a.n_phys) atomicAdd(&s_cur[key_range(k[q], a)], 1u);
+        if (li + q >= lo && li + q < hi) atomicAdd(&s_cur[key_range(k[q], a)], 1u);
     }
     __syncthreads();
     if (threadIdx.x < 32) {
@@ -158,26 +165,27 @@ static __global__ void __launch_bounds__(kPartThreads, 8) part_scatter_kernel(co
     __syncthreads();
 #pragma unroll
     for (int i = 0; i < kPartKeysPerThread / 4; i++) {
-      const uint64_t p0 = (v0 + static_cast<uint64_t>(i) * kPartThreads + threadIdx.x) * 4;
-      const uint32_t k[4] = {kv[i].x, kv[i].y, kv[i].z, kv[i].w};
+      const uint32_t li = (i * kPartThreads + threadIdx.x) * 4;
+      const uint4 x = li < hi ? __ldcs(t4 + li / 4) : make_uint4(0, 0, 0, 0);
+      const uint32_t k[4] = {x.x, x.y, x.z, x.w};
 #pragma unroll
       for (int q = 0; q < 4; q++) {
-        if (p0 + q >= a.pre && p0 + q < a.n_phys) {
+        if (li + q >= lo && li + q < hi) {
           const uint32_t slot = atomicAdd(&s_cur[key_range(k[q], a)], 1u);
           s_keys[slot] = k[q];
-          s_idx[slot] = static_cast<uint16_t>((i * kPartThreads + threadIdx.x) * 4 + q);
+          s_idx[slot] = static_cast<uint16_t>(li + q);
         }
       }
     }
     __syncthreads();
     const uint32_t nv = s_valid;
-    const uint64_t tile_pos = static_cast<uint64_t>(tile) * kPartTile;  // physical index of the tile's key 0
+    const uint32_t pos0 = static_cast<uint32_t>(tile_pos - a.pre);  // logical position of tile index 0 (mod 2^32)
     for (uint32_t sl = threadIdx.x; sl < nv; sl += blockDim.x) {
       const uint32_t key = s_keys[sl];
       const uint32_t r = key_range(key, a);
-      const uint64_t g = static_cast<uint64_t>(s_gbase[r]) + (sl - s_lbase[r]);
+      const uint32_t g = s_gbase[r] + (sl - s_lbase[r]);
       const uint64_t cap = r + 1 < a.n_ranges ? a.seg_cap : a.last_cap;
-      const uint2 pr = make_uint2(key, static_cast<uint32_t>(tile_pos + s_idx[sl] - a.pre));
+      const uint2 pr = make_uint2(key, pos0 + s_idx[sl]);
       if (g < cap) {
         __stcs(a.pairs + static_cast<uint64_t>(r) * a.seg_cap + g, pr);
       } else {
@@ -198,7 +206,7 @@ struct SegChunks {
   const uint2* pairs;
   uint64_t seg_cap, last_cap;
   uint32_t n_ranges;
-  uint32_t chunks_per_seg;  // seg_cap / kPartChunk
+  uint32_t chunks_per_seg;  // seg_cap / kPartChunk (a segment holds < 2^32 pairs)
   uint32_t n_chunks;        // (n_ranges - 1) * chunks_per_seg + last_cap / kPartChunk
   const PartHeader* hdr;
 };
@@ -215,33 +223,34 @@ __host__ __device__ inline SegChunks seg_chunks(const PartArgs& pa) {
   return s;
 }
 
-// Pairs of chunk c: first pair and count (0 .. kPartChunk).
-__device__ __forceinline__ uint32_t chunk_pairs(const SegChunks& s, uint32_t c, uint64_t* first) {
-  uint32_t r = c / s.chunks_per_seg;
-  if (r >= s.n_ranges) r = s.n_ranges - 1;
-  const uint64_t j0 = static_cast<uint64_t>(c - r * s.chunks_per_seg) * kPartChunk;
-  const uint64_t cap = r + 1 < s.n_ranges ? s.seg_cap : s.last_cap;
-  const uint64_t fill = s.hdr->fill[r];
-  const uint64_t filled = fill < cap ? fill : cap;
-  *first = static_cast<uint64_t>(r) * s.seg_cap + j0;
-  if (filled <= j0) return 0u;
-  return filled - j0 < kPartChunk ? static_cast<uint32_t>(filled - j0) : kPartChunk;
-}
-
 // Runs fn(key, position) over every pair of the segments: each CTA takes
 // whole chunks, the grid sweeping them in range order, so the CTAs in flight
-// work on one or two ranges at a time.  One 8-byte pair per thread and step
-// (two per 16-byte load needed more registers than the 32-register pair
-// probe has).
+// work on one or two ranges at a time.  The ranges' fill counts are read into
+// shared memory once per CTA, so a chunk starts without a global load; pairs
+// are read two per 16-byte load.
 template <class Fn>
 __device__ __forceinline__ void for_each_pair(const SegChunks& s, Fn fn) {
+  __shared__ uint32_t s_filled[kMaxRanges];  // pairs in each segment (fill, capped at the capacity)
+  for (uint32_t r = threadIdx.x; r < s.n_ranges; r += blockDim.x) {
+    const uint64_t cap = r + 1 < s.n_ranges ? s.seg_cap : s.last_cap;
+    const uint32_t fill = s.hdr->fill[r];
+    s_filled[r] = fill < cap ? fill : static_cast<uint32_t>(cap);
+  }
+  __syncthreads();
+  const uint4* p4 = reinterpret_cast<const uint4*>(s.pairs);
+  const uint64_t half_seg = s.seg_cap >> 1;  // 16-byte vectors per segment
   for (uint32_t c = blockIdx.x; c < s.n_chunks; c += gridDim.x) {
-    uint64_t first = 0;
-    const uint32_t cnt = chunk_pairs(s, c, &first);
-    const uint2* p = s.pairs + first;
-    for (uint32_t j = threadIdx.x; j < cnt; j += blockDim.x) {
-      const uint2 x = __ldcs(p + j);
+    uint32_t r = c / s.chunks_per_seg;
+    if (r >= s.n_ranges) r = s.n_ranges - 1;
+    const uint32_t j0 = (c - r * s.chunks_per_seg) * kPartChunk;
+    const uint32_t filled = s_filled[r];
+    if (filled <= j0) continue;
+    const uint32_t cnt = filled - j0 < kPartChunk ? filled - j0 : kPartChunk;
+    const uint4* q = p4 + static_cast<uint64_t>(r) * half_seg + (j0 >> 1);
+    for (uint32_t v = threadIdx.x; 2 * v < cnt; v += blockDim.x) {
+      const uint4 x = __ldcs(q + v);
       fn(x.x, x.y);
+      if (2 * v + 1 < cnt) fn(x.z, x.w);
     }
   }
 }
