@@ -59,6 +59,7 @@ struct PartHeader {
   unsigned int fill[kMaxRanges];     // pairs requested per range (may exceed the capacity)
   unsigned int overflow_tiles;       // tiles with at least one overflowing run
   unsigned int spill_cnt;            // pairs in the spill list
+  unsigned int chunk_ctr;            // next chunk of the segments to hand out (pair kernels)
 };
 static_assert(sizeof(PartHeader) <= kPartHeaderBytes, "partition header");
 
@@ -223,23 +224,31 @@ __host__ __device__ inline SegChunks seg_chunks(const PartArgs& pa) {
   return s;
 }
 
-// Runs fn(key, position) over every pair of the segments: each CTA takes
-// whole chunks, the grid sweeping them in range order, so the CTAs in flight
-// work on one or two ranges at a time.  The ranges' fill counts are read into
-// shared memory once per CTA, so a chunk starts without a global load; pairs
-// are read two per 16-byte load.
+// Runs fn(key, position) over every pair of the segments: CTAs take whole
+// chunks from a queue (one atomic per chunk), in range order, so the chunks in
+// flight are the ones next to each other and the filter range they read stays
+// in L2 (a fixed grid-stride assignment lets slow and fast CTAs drift apart
+// over two or more ranges, whose words then evict each other).  The ranges'
+// fill counts are read into shared memory once per CTA; pairs are read two
+// per 16-byte load.  The queue counter (PartHeader::chunk_ctr) must be zero.
 template <class Fn>
 __device__ __forceinline__ void for_each_pair(const SegChunks& s, Fn fn) {
   __shared__ uint32_t s_filled[kMaxRanges];  // pairs in each segment (fill, capped at the capacity)
+  __shared__ uint32_t s_chunk;
   for (uint32_t r = threadIdx.x; r < s.n_ranges; r += blockDim.x) {
     const uint64_t cap = r + 1 < s.n_ranges ? s.seg_cap : s.last_cap;
     const uint32_t fill = s.hdr->fill[r];
     s_filled[r] = fill < cap ? fill : static_cast<uint32_t>(cap);
   }
-  __syncthreads();
   const uint4* p4 = reinterpret_cast<const uint4*>(s.pairs);
   const uint64_t half_seg = s.seg_cap >> 1;  // 16-byte vectors per segment
-  for (uint32_t c = blockIdx.x; c < s.n_chunks; c += gridDim.x) {
+  unsigned int* ctr = const_cast<unsigned int*>(&s.hdr->chunk_ctr);
+  for (;;) {
+    if (threadIdx.x == 0) s_chunk = atomicAdd(ctr, 1u);
+    __syncthreads();
+    const uint32_t c = s_chunk;
+    __syncthreads();  // s_chunk is rewritten for the next chunk
+    if (c >= s.n_chunks) break;
     uint32_t r = c / s.chunks_per_seg;
     if (r >= s.n_ranges) r = s.n_ranges - 1;
     const uint32_t j0 = (c - r * s.chunks_per_seg) * kPartChunk;
