@@ -54,6 +54,7 @@ struct dtlg_batch {
   std::vector<dtlg_batch_item> items;
   std::vector<BatchDesc> desc;       // host copy (with staging as planned at prepare)
   uint32_t* d_bucket = nullptr;      // all staged filters' range buckets
+  uint32_t* d_mask = nullptr;        // all filters' match bitmasks
   uint2* d_items[2] = {nullptr, nullptr};  // the queue with staged builds [0] / all direct [1]
   uint32_t n_items[2] = {0, 0};
   size_t ranges_built_off = 0, cursor_off = 0;
@@ -61,10 +62,10 @@ struct dtlg_batch {
   std::vector<int> fallback;         // item indexes run as separate launches
   std::vector<void*> fallback_ws;
   std::vector<size_t> fallback_ws_bytes;
-  uint32_t n_menu = 0, n_probe_tiles = 0;
+  uint32_t n_menu = 0, n_probe_tiles = 0, n_ctiles = 0;
   BatchDesc* d_desc = nullptr;
-  char* d_ctl = nullptr;             // ctl words | built counters | status words
-  size_t ctl_bytes = 0, built_off = 0, status_off = 0;
+  char* d_ctl = nullptr;             // ctl words | built / ranges / probed counters | cursors | status words
+  size_t ctl_bytes = 0, built_off = 0, probed_off = 0, status_off = 0;
   int sms = 0, occupancy = 1, ctas_per_sm = 0;
   bool use_graph = false;
   bool warm = false;
@@ -84,6 +85,7 @@ dtlg_status enqueue(dtlg_batch* b, cudaStream_t s) {
     a.ctl = reinterpret_cast<unsigned int*>(b->d_ctl);
     a.built = reinterpret_cast<unsigned int*>(b->d_ctl + b->built_off);
     a.ranges_built = reinterpret_cast<unsigned int*>(b->d_ctl + b->ranges_built_off);
+    a.probed = reinterpret_cast<unsigned int*>(b->d_ctl + b->probed_off);
     a.items = b->d_items[b->staging == 1 ? 1 : 0];
     a.n_items = b->n_items[b->staging == 1 ? 1 : 0];
     a.status = reinterpret_cast<unsigned long long*>(b->d_ctl + b->status_off);
@@ -112,6 +114,7 @@ void release(dtlg_batch* b) {
   cudaFree(b->d_desc);
   cudaFree(b->d_ctl);
   cudaFree(b->d_bucket);
+  cudaFree(b->d_mask);
   cudaFree(b->d_items[0]);
   cudaFree(b->d_items[1]);
   for (void* p : b->fallback_ws) cudaFree(p);
@@ -139,7 +142,9 @@ dtlg_status dtlg_batch_prepare(const dtlg_batch_item* items, uint32_t n_items, i
   b->items.assign(items, items + n_items);
   b->use_graph = use_graph != 0;
   std::vector<BatchDesc> desc;
-  uint32_t n_probe_tiles = 0;
+  uint32_t n_probe_tiles = 0, n_ctiles = 0;
+  size_t mask_words = 0;
+  std::vector<size_t> mask_at;
   for (uint32_t i = 0; i < n_items; i++) {
     const dtlg_batch_item& it = items[i];
     if (!it.filter || !it.filter_words || !it.match_cnt || (it.n_build && !it.build_keys) ||
@@ -174,6 +179,11 @@ dtlg_status dtlg_batch_prepare(const dtlg_batch_item* items, uint32_t n_items, i
     d.probe_tile0 = n_probe_tiles;
     d.n_probe_tiles = tiles_of(it.n_probe);
     n_probe_tiles += d.n_probe_tiles;
+    d.ctile0 = n_ctiles;
+    d.n_ctiles = static_cast<uint32_t>((static_cast<uint64_t>(it.n_probe) + kBatchCompactKeys - 1) / kBatchCompactKeys);
+    n_ctiles += d.n_ctiles;
+    mask_at.push_back(mask_words);
+    mask_words += (static_cast<size_t>(it.n_probe) + 127) / 128 * 4;  // 16-byte aligned per filter
     const uint32_t f = static_cast<uint32_t>(desc.size());
     desc.push_back(d);
   }
@@ -219,24 +229,31 @@ dtlg_status dtlg_batch_prepare(const dtlg_batch_item* items, uint32_t n_items, i
     for (uint32_t f = 0; f < nf; f++)
       for (uint32_t t = 0; t < desc[f].n_probe_tiles; t++)
         queue[v].push_back(make_uint2((kItemProbe << 30) | f, desc[f].probe_tile0 + t));
+    for (uint32_t f = 0; f < nf; f++)
+      for (uint32_t t = 0; t < desc[f].n_ctiles; t++)
+        queue[v].push_back(make_uint2((kItemCompact << 30) | f, desc[f].ctile0 + t));
     b->n_items[v] = static_cast<uint32_t>(queue[v].size());
   }
   b->n_menu = static_cast<uint32_t>(desc.size());
   b->n_probe_tiles = n_probe_tiles;
+  b->n_ctiles = n_ctiles;
   b->built_off = 256;
   b->ranges_built_off = b->built_off + round256(static_cast<size_t>(b->n_menu) * 4);
-  b->cursor_off = b->ranges_built_off + round256(static_cast<size_t>(b->n_menu) * 4);
+  b->probed_off = b->ranges_built_off + round256(static_cast<size_t>(b->n_menu) * 4);
+  b->cursor_off = b->probed_off + round256(static_cast<size_t>(b->n_menu) * 4);
   b->status_off = b->cursor_off + round256(cursor_words * 4);
-  b->ctl_bytes = b->status_off + round256(static_cast<size_t>(b->n_probe_tiles) * 8);
+  b->ctl_bytes = b->status_off + round256(static_cast<size_t>(b->n_ctiles) * 8);
   if (ok && b->n_menu) {
     ok = cudaMalloc(&b->d_ctl, b->ctl_bytes) == cudaSuccess &&
          cudaMalloc(&b->d_bucket, std::max<size_t>(1, bucket_words) * 4) == cudaSuccess &&
+         cudaMalloc(&b->d_mask, std::max<size_t>(1, mask_words) * 4) == cudaSuccess &&
          cudaMalloc(&b->d_items[0], std::max<size_t>(1, queue[0].size()) * sizeof(uint2)) == cudaSuccess &&
          cudaMalloc(&b->d_items[1], std::max<size_t>(1, queue[1].size()) * sizeof(uint2)) == cudaSuccess &&
          (queue[0].empty() || cudaMemcpy(b->d_items[0], queue[0].data(), queue[0].size() * sizeof(uint2),
                                          cudaMemcpyHostToDevice) == cudaSuccess) &&
          (queue[1].empty() || cudaMemcpy(b->d_items[1], queue[1].data(), queue[1].size() * sizeof(uint2),
                                          cudaMemcpyHostToDevice) == cudaSuccess);
+    for (size_t f = 0; ok && f < desc.size(); f++) desc[f].mask = b->d_mask + mask_at[f];
     for (size_t f = 0; ok && f < desc.size(); f++) {
       if (!desc[f].staged) continue;
       desc[f].bucket = b->d_bucket + bucket_at[f];

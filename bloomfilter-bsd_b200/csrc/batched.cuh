@@ -5,13 +5,20 @@
 // most of the time on launch latency and tail effects.  Here all filters are
 // described by a table, and one persistent kernel works through a queue of three kinds of items:
 //
-//   build tiles: 4096 build keys of one filter;
-//   range items: one block range of a staged filter;
-//   probe tiles: 4096 probe keys of one filter, each filter's tiles in order
-//                (per-filter ordered compaction).
+//   build tiles:   4096 build keys of one filter;
+//   range items:   one block range of a staged filter;
+//   probe tiles:   4096 probe keys of one filter, tested into the filter's
+//                  key-ordered match bitmask (128 words, no barrier between
+//                  the warps, no look-back);
+//   compact tiles: 65536 keys of one filter: ordered compaction of its
+//                  bitmask into ascending match positions (per-filter
+//                  decoupled look-back, as compact_kernel in probe2.cuh).
 //
 // The items form one queue: all build tiles, then all range items, then all
-// probe tiles, each kind in filter order.
+// probe tiles, then all compact tiles, each kind in filter order.  (Probing
+// into a bitmask and compacting separately, as the single-filter plan 2 does,
+// is 2.2x the rate of a fused probe-and-compact tile on B200: u64 w=8 s=8 k=8,
+// 2^22 keys, 2^28 probes, 183 vs 83 Gkeys/s.)
 //
 // A build tile either inserts its keys with global atomic ORs (direct
 // filters), or -- for a staged filter -- only sorts them into per-range
@@ -55,7 +62,9 @@ struct BatchDesc {
   unsigned long long* count_out;
   uint32_t n_build, n_probe, match_offset;
   uint32_t n_build_tiles;               // build tiles of this filter
-  uint32_t probe_tile0, n_probe_tiles;  // first global probe tile (look-back word), tile count
+  uint32_t probe_tile0, n_probe_tiles;  // first global probe tile, tile count
+  uint32_t ctile0, n_ctiles;            // first global compact tile (look-back word), tile count
+  uint32_t* mask;                       // match bitmask, one bit per probe key (whole 128-word tiles)
   // staged build (staged != 0): range r holds blocks [r << range_shift, ...)
   uint32_t staged, n_ranges, range_shift, bucket_cap;
   uint32_t* bucket;             // n_ranges x bucket_cap keys
@@ -65,14 +74,17 @@ struct BatchDesc {
 // Work items of the single queue: x = kind << 30 | filter, y = the kind's index.
 constexpr uint32_t kItemBuild = 0;   // y: the filter's build tile
 constexpr uint32_t kItemRange = 1;   // y: the range of a staged filter
-constexpr uint32_t kItemProbe = 2;   // y: the global probe tile (look-back word)
+constexpr uint32_t kItemProbe = 2;   // y: the global probe tile
+constexpr uint32_t kItemCompact = 3; // y: the global compact tile (look-back word)
+constexpr uint32_t kBatchCompactKeys = 65536;  // keys per compact tile: 8 warps x 8 rows x 32 words
 
 struct BatchArgs {
   const BatchDesc* desc;
   uint32_t n_filters;
   const uint2* items;           // the queue, in hand-out order
   uint32_t n_items;
-  unsigned long long* status;   // one look-back word per global probe tile (zeroed)
+  unsigned long long* status;   // one look-back word per global compact tile (zeroed)
+  unsigned int* probed;         // per filter: probe tiles done (zeroed)
   unsigned int* built;          // per filter: build tiles done (zeroed)
   unsigned int* ranges_built;   // per filter: range items done (zeroed)
   unsigned int* ctl;            // [0] queue head, [2] error word (zeroed)
@@ -258,7 +270,6 @@ __global__ void __launch_bounds__(kBatchThreads, 4) batched_kernel(const __grid_
   __shared__ uint32_t s_excl;
   extern __shared__ __align__(16) unsigned char s_dyn[];  // kBatchRangeBytes
   const uint32_t lane = threadIdx.x & 31u, warp = threadIdx.x >> 5;
-  const uint32_t lt_mask = (1u << lane) - 1u;
 
   // filters without probe keys report a zero count
   if (blockIdx.x == 0) {
@@ -318,99 +329,133 @@ __global__ void __launch_bounds__(kBatchThreads, 4) batched_kernel(const __grid_
       continue;
     }
 
-    // kItemProbe
-    const uint32_t tile = it.y;
-    const uint32_t local = tile - d.probe_tile0;
-    if (d.staged) {
-      wait_counter(&a.ranges_built[f], d.n_ranges, &a.ctl[2]);
-    } else {
-      wait_counter(&a.built[f], d.n_build_tiles, &a.ctl[2]);
-    }
-    const uint64_t k0 = static_cast<uint64_t>(local) * kBatchTile;
-    uint32_t flags[kRounds];
-    uint32_t lane_excl[kRounds];
-    // blocks of >= 32 bytes are read with 256-bit loads when the words are 32-byte aligned
-    const bool vec32 = (reinterpret_cast<uintptr_t>(d.words) & 31u) == 0;
-    dispatch_cfg<Cfgs...>(d.cfg, [&](auto c) {
-      using Cfg = decltype(c);
-      const uint4* k4 = reinterpret_cast<const uint4*>(d.probe_keys + k0);
+    if (kind == kItemProbe) {
+      const uint32_t tile = it.y;
+      const uint32_t local = tile - d.probe_tile0;
+      if (d.staged) {
+        wait_counter(&a.ranges_built[f], d.n_ranges, &a.ctl[2]);
+      } else {
+        wait_counter(&a.built[f], d.n_build_tiles, &a.ctl[2]);
+      }
+      const uint64_t k0 = static_cast<uint64_t>(local) * kBatchTile;
+      const uint32_t n_words = (d.n_probe + 31u) / 32u;
+      // blocks of >= 32 bytes are read with 256-bit loads when the words are 32-byte aligned
+      const bool vec32 = (reinterpret_cast<uintptr_t>(d.words) & 31u) == 0;
+      dispatch_cfg<Cfgs...>(d.cfg, [&](auto c) {
+        using Cfg = decltype(c);
+        const uint4* k4 = reinterpret_cast<const uint4*>(d.probe_keys + k0);
 #pragma unroll
-      for (int r = 0; r < kRounds; r++) {
-        const uint64_t i0 = static_cast<uint64_t>(r) * (kBatchThreads * 4) + threadIdx.x * 4u;
-        uint32_t fl = 0;
-        if (k0 + i0 < d.n_probe) {
-          const uint4 kv = __ldcs(k4 + (i0 >> 2));
-          const uint32_t k[4] = {kv.x, kv.y, kv.z, kv.w};
+        for (int r = 0; r < kRounds; r++) {
+          const uint32_t i0 = r * (kBatchThreads * 4) + threadIdx.x * 4u;
+          uint32_t fl = 0;
+          if (k0 + i0 < d.n_probe) {
+            const uint4 kv = __ldcs(k4 + (i0 >> 2));
+            const uint32_t k[4] = {kv.x, kv.y, kv.z, kv.w};
 #pragma unroll
-          for (int q = 0; q < 4; q++) {
-            const uint32_t blk = block_index(k[q] * mul_const(0), d.addr);
-            const auto* base = static_cast<const typename Cfg::word_t*>(d.words) +
-                               static_cast<uint64_t>(blk) * Cfg::kW;
-            const bool hit = BloomOps<Cfg>::template test_block<false>(base, k[q], vec32);
-            fl |= ((hit && k0 + i0 + q < d.n_probe) ? 1u : 0u) << q;
+            for (int q = 0; q < 4; q++) {
+              const uint32_t blk = block_index(k[q] * mul_const(0), d.addr);
+              const auto* base = static_cast<const typename Cfg::word_t*>(d.words) +
+                                 static_cast<uint64_t>(blk) * Cfg::kW;
+              const bool hit = BloomOps<Cfg>::template test_block<false>(base, k[q], vec32);
+              fl |= ((hit && k0 + i0 + q < d.n_probe) ? 1u : 0u) << q;
+            }
           }
+          // lanes 8j .. 8j+7 hold keys 32j .. 32j+31 of the warp's 128: word j
+          uint32_t x = fl << (4u * (lane & 7u));
+          x |= __shfl_xor_sync(0xffffffffu, x, 1);
+          x |= __shfl_xor_sync(0xffffffffu, x, 2);
+          x |= __shfl_xor_sync(0xffffffffu, x, 4);
+          const uint32_t w = local * (kBatchTile / 32) + r * (kBatchThreads * 4 / 32) + warp * 4 + (lane >> 3);
+          if ((lane & 7u) == 0 && w < n_words) __stcg(d.mask + w, x);
         }
-        flags[r] = fl;
+      });
+      __syncthreads();
+      if (threadIdx.x == 0) {
+        __threadfence();
+        atomicAdd(&a.probed[f], 1u);
       }
-    });
-#pragma unroll
-    for (int r = 0; r < kRounds; r++) {
-      uint32_t tot = 0, ex = 0;
-#pragma unroll
-      for (int q = 0; q < 4; q++) {
-        const uint32_t b = __ballot_sync(0xffffffffu, (flags[r] >> q) & 1u);
-        ex += __popc(b & lt_mask);
-        tot += __popc(b);
-      }
-      lane_excl[r] = ex;
-      if (lane == 0) s_wtot[r * kWarps + warp] = tot;
+      continue;
     }
+
+    // kItemCompact: ordered compaction of 65536 keys' match bits.  Warp w owns
+    // the 256 words w*256 .. w*256+255 of the tile as 8 rows of 32 (lane l
+    // holds word row*32 + l); the tile's offset comes from the look-back over
+    // this filter's compact tiles, the warp's from a CTA scan, a row's from a
+    // warp scan; a row's matches are staged in shared memory in key order and
+    // stored by the whole warp to consecutive slots.
+    const uint32_t ct = it.y;
+    const uint32_t local = ct - d.ctile0;
+    wait_counter(&a.probed[f], d.n_probe_tiles, &a.ctl[2]);
+    constexpr int kRows = 8;
+    const uint32_t n_words = (d.n_probe + 31u) / 32u;
+    const uint64_t wbase = static_cast<uint64_t>(local) * (kBatchCompactKeys / 32) + warp * (kRows * 32);
+    uint32_t wv[kRows];
+    uint32_t cnt = 0;
+#pragma unroll
+    for (int i = 0; i < kRows; i++) {
+      const uint64_t idx = wbase + static_cast<uint64_t>(i) * 32 + lane;
+      wv[i] = idx < n_words ? __ldcg(d.mask + idx) : 0u;
+      cnt += __popc(wv[i]);
+    }
+#pragma unroll
+    for (int dd = 16; dd > 0; dd >>= 1) cnt += __shfl_xor_sync(0xffffffffu, cnt, dd);
+    if (lane == 0) s_wtot[warp] = cnt;
     __syncthreads();
     if (warp == 0) {
-      const uint32_t v = lane < kRounds * kWarps ? s_wtot[lane] : 0u;
-      uint32_t incl = v;
+      const uint32_t v = lane < kWarps ? s_wtot[lane] : 0u;
+      uint32_t wi = v;
 #pragma unroll
-      for (int dd = 1; dd < 32; dd <<= 1) {
-        const uint32_t t = __shfl_up_sync(0xffffffffu, incl, dd);
-        if (lane >= static_cast<uint32_t>(dd)) incl += t;
+      for (int dd = 1; dd < kWarps; dd <<= 1) {
+        const uint32_t t = __shfl_up_sync(0xffffffffu, wi, dd);
+        if (lane >= static_cast<uint32_t>(dd)) wi += t;
       }
-      const uint32_t agg = __shfl_sync(0xffffffffu, incl, 31);
-      if (lane < kRounds * kWarps) s_wtot[lane] = incl - v;
+      const uint32_t agg = __shfl_sync(0xffffffffu, wi, kWarps - 1);
+      if (lane < kWarps) s_wtot[lane] = wi - v;
       uint32_t excl = 0;
       if (local == 0) {
-        if (lane == 0) st_volatile(a.status + tile, kFlagPrefix | agg);
+        if (lane == 0) st_volatile(a.status + ct, kFlagPrefix | agg);
       } else {
-        if (lane == 0) st_volatile(a.status + tile, kFlagAgg | agg);
-        // look back over this filter's earlier tiles only (global tiles
-        // probe_tile0 .. tile-1): the helper sees a status array that
-        // starts at this filter's first tile
+        if (lane == 0) st_volatile(a.status + ct, kFlagAgg | agg);
+        // look back over this filter's earlier compact tiles only
         ProbeArgs fl = lb;
-        fl.status = a.status + d.probe_tile0;
+        fl.status = a.status + d.ctile0;
         excl = look_back(fl, local, lane);
-        if (lane == 0) st_volatile(a.status + tile, kFlagPrefix | static_cast<uint32_t>(excl + agg));
+        if (lane == 0) st_volatile(a.status + ct, kFlagPrefix | static_cast<uint32_t>(excl + agg));
       }
       if (lane == 0) {
         s_excl = excl;
-        if (local == d.n_probe_tiles - 1) {
+        if (local == d.n_ctiles - 1) {
           const bool failed = *reinterpret_cast<volatile unsigned int*>(&a.ctl[2]) != 0u;
           *d.count_out = failed ? ~0ull : static_cast<unsigned long long>(excl) + agg;
         }
       }
     }
     __syncthreads();
-    const uint32_t excl = s_excl;
+    uint32_t pos = s_excl + s_wtot[warp];
+    uint32_t* stage = reinterpret_cast<uint32_t*>(s_dyn) + warp * 1024;  // 8 x 4 KiB of the 32 KiB
 #pragma unroll
-    for (int r = 0; r < kRounds; r++) {
-      uint32_t fl = flags[r];
-      if (fl == 0) continue;
-      uint32_t pos = excl + s_wtot[r * kWarps + warp] + lane_excl[r];
-      const uint32_t i0 = static_cast<uint32_t>(k0) + r * (kBatchThreads * 4) + threadIdx.x * 4u;
-      while (fl) {
-        const int q = __ffs(fl) - 1;
-        fl &= fl - 1;
-        __stcs(d.out + pos, i0 + static_cast<uint32_t>(q) + d.match_offset);
-        pos++;
+    for (int i = 0; i < kRows; i++) {
+      const uint32_t ci = __popc(wv[i]);
+      uint32_t incl = ci;
+#pragma unroll
+      for (int dd = 1; dd < 32; dd <<= 1) {
+        const uint32_t t = __shfl_up_sync(0xffffffffu, incl, dd);
+        if (lane >= static_cast<uint32_t>(dd)) incl += t;
       }
+      const uint32_t tot = __shfl_sync(0xffffffffu, incl, 31);
+      if (tot == 0) continue;
+      const uint32_t first = static_cast<uint32_t>((wbase + static_cast<uint64_t>(i) * 32 + lane) * 32);
+      uint32_t m = wv[i];
+      uint32_t o = incl - ci;
+      while (m) {
+        const uint32_t b = __ffs(m) - 1;
+        m &= m - 1;
+        stage[o++] = first + b;
+      }
+      __syncwarp();
+      for (uint32_t j = lane; j < tot; j += 32) __stcs(d.out + pos + j, stage[j] + d.match_offset);
+      __syncwarp();
+      pos += tot;
     }
     __syncthreads();
   }
