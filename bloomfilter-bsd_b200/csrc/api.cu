@@ -257,20 +257,18 @@ int probe_plan(const dtlg_filter* f, uint64_t n) {
 // 85.3 / 80.4 with 32 MiB ranges, 92.2 / 94.3 / 89.0 against 89.7 / 92.1 /
 // 90.5 with 8 MiB ranges; zoned u64 w=8 z=2 at 256 / 384 MiB 94.4 / 91.1
 // against 92.7 / 88.3.
-// A 32-register variant that spills (local memory per thread, from
-// cudaFuncGetAttributes) gives way to the 64-register one: -Xptxas -v shows
-// spills in the pair probe of 4 layouts with k = 16 and in the bitmask kernel
-// of 19 layouts, none of them among the layouts the rule above was measured on.
+// A 32-register bitmask kernel that spills (local memory per thread, from
+// cudaFuncGetAttributes; -Xptxas -v: 19 layouts) gives way to the 64-register
+// one: u64 w=1 k=16 at 200 MiB, 2^27 probes, spilling v0 65.1 against v1 69.3
+// Gkeys/s.  The pair probe keeps v0 where it spills (7 layouts, all k >= 12):
+// its spills cost less than the halved occupancy of v1 (u64 w=8 s=8 k=16 at
+// 512 MiB: 83.0 against 79.7; u64 w=4 s=4 k=16 at 192 MiB: 89.7 against 87.5).
 int probe_variant(const dtlg_filter* f, int mode) {
   if (f->bits_variant >= 0 && f->bits_variant < kBitsVariants) return f->bits_variant;
-  int v;
-  if (mode == 3) {
-    v = (f->d.kind == Kind::kBloom || f->d.kind == Kind::kZoned) ? 0 : 1;
-  } else {
-    v = bitmask_band(f) ? 0 : 1;
-  }
+  if (mode == 3) return (f->d.kind == Kind::kBloom || f->d.kind == Kind::kZoned) ? 0 : 1;
+  int v = bitmask_band(f) ? 0 : 1;
   if (v == 0) {
-    const occ_fn spill = mode == 3 ? f->pk->pairs_local_bytes[0] : f->pk->bits_local_bytes[0];
+    const occ_fn spill = f->pk->bits_local_bytes[0];
     if (spill && spill() != 0) v = 1;
   }
   return v;
@@ -370,7 +368,14 @@ dtlg_status launch_probe(const dtlg_filter* f, const uint64_t* words, const uint
   a.err = &h->err;
   a.n_tiles = tiles;
   set_filter_args(f->d, &a);
+  // blocks of >= 32 bytes are read with 256-bit loads when the words are
+  // 32-byte aligned (every plan; the fused plan read them as two 128-bit
+  // loads before, which doubled its L1 wavefronts)
+  a.vec32 = (reinterpret_cast<uintptr_t>(words) & 31u) == 0 ? 1u : 0u;
   if (mode == 1) {
+    // the fused plan reads Bloom filters that cannot live in L1 without
+    // allocating there, as the bitmask plan does (below)
+    a.l1na = (f->bk != nullptr && (f->d.m_actual / 8) > kL1NoAllocBytes) ? 1u : 0u;
     const probe_fn fn = f->pk->probe;
     const occ_fn occ = f->pk->probe_blocks_per_sm;
     const int per_sm = std::max(1, occ());
@@ -380,7 +385,6 @@ dtlg_status launch_probe(const dtlg_filter* f, const uint64_t* words, const uint
   }
   uint32_t* bits = reinterpret_cast<uint32_t*>(wsb + lay.bits_off);
   const int v = probe_variant(f, mode);
-  a.vec32 = (reinterpret_cast<uintptr_t>(words) & 31u) == 0 ? 1u : 0u;
   if (mode == 4) {
     // the whole filter in every CTA's shared memory
     const uint32_t words32 = static_cast<uint32_t>((f->d.m_actual + 31) / 32);

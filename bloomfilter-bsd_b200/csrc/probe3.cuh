@@ -104,14 +104,16 @@ __device__ __forceinline__ uint32_t key_range(uint32_t key, const PartArgs& a) {
 // each range in its segment (one global atomic per tile and range), sort the
 // tile by range in shared memory and write every run with consecutive
 // addresses.  Shared memory holds the sorted keys and their 12-bit tile
-// positions (24 KiB), so eight CTAs fit on an SM.  Inside a tile all index
-// arithmetic is 32-bit.
+// positions (24 KiB), so eight CTAs fit on an SM.  The kernel is bound by
+// instruction issue, so the tile's index arithmetic is 32-bit, a key's range
+// is computed once for the count and the placement (kept as bytes), and each
+// range's destination base and slot limit are computed once per tile.
 static __global__ void __launch_bounds__(kPartThreads, 8) part_scatter_kernel(const __grid_constant__ PartArgs a) {
   __shared__ uint32_t s_keys[kPartTile];
   __shared__ uint16_t s_idx[kPartTile];
   __shared__ uint32_t s_cur[kMaxRanges];    // counts, then the placement cursor
-  __shared__ uint32_t s_lbase[kMaxRanges];  // tile-local start of each range's run
-  __shared__ uint32_t s_gbase[kMaxRanges];  // the run's first slot in its segment
+  __shared__ uint32_t s_lim[kMaxRanges];    // sorted slots below this go to the segment, the rest overflow
+  __shared__ unsigned long long s_dst[kMaxRanges];  // pair index of sorted slot 0 for the range's run
   __shared__ uint32_t s_valid;
   __shared__ unsigned long long s_over;
   const uint4* keys4 = reinterpret_cast<const uint4*>(a.keys_al);
@@ -126,25 +128,34 @@ static __global__ void __launch_bounds__(kPartThreads, 8) part_scatter_kernel(co
     const uint32_t hi = a.n_phys - tile_pos < kPartTile ? static_cast<uint32_t>(a.n_phys - tile_pos) : kPartTile;
     const uint4* t4 = keys4 + tile_pos / 4;
     // the keys are read twice: for the counts and, from L2, for the placement
-    // (holding them across the scan would not fit 32 registers)
-    uint4 kv[kPartKeysPerThread / 4];
+    // (holding them across the scan would not fit 32 registers); their ranges
+    // are kept, four bytes per register
+    uint32_t rr[kPartKeysPerThread / 4];
+    {
+      uint4 kv[kPartKeysPerThread / 4];
 #pragma unroll
-    for (int i = 0; i < kPartKeysPerThread / 4; i++) {
-      const uint32_t li = (i * kPartThreads + threadIdx.x) * 4;
-      kv[i] = li < hi ? __ldcg(t4 + li / 4) : make_uint4(0, 0, 0, 0);
-    }
+      for (int i = 0; i < kPartKeysPerThread / 4; i++) {
+        const uint32_t li = (i * kPartThreads + threadIdx.x) * 4;
+        kv[i] = li < hi ? __ldcg(t4 + li / 4) : make_uint4(0, 0, 0, 0);
+      }
 #pragma unroll
-    for (int i = 0; i < kPartKeysPerThread / 4; i++) {
-      const uint32_t li = (i * kPartThreads + threadIdx.x) * 4;
-      const uint32_t k[4] = {kv[i].x, kv[i].y, kv[i].z, kv[i].w};
+      for (int i = 0; i < kPartKeysPerThread / 4; i++) {
+        const uint32_t li = (i * kPartThreads + threadIdx.x) * 4;
+        const uint32_t k[4] = {kv[i].x, kv[i].y, kv[i].z, kv[i].w};
+        rr[i] = 0;
 #pragma unroll
-      for (int q = 0; q < 4; q++)
-        if (li + q >= lo && li + q < hi) atomicAdd(&s_cur[key_range(k[q], a)], 1u);
+        for (int q = 0; q < 4; q++) {
+          const uint32_t r = key_range(k[q], a);
+          rr[i] |= r << (8 * q);
+          if (li + q >= lo && li + q < hi) atomicAdd(&s_cur[r], 1u);
+        }
+      }
     }
     __syncthreads();
     if (threadIdx.x < 32) {
-      // tile-local run starts (exclusive scan, two ranges per lane) and the
-      // runs' slots in their segments
+      // tile-local run starts (exclusive scan, two ranges per lane), the runs'
+      // slots in their segments, and per range the destination of sorted slot
+      // 0 and the first sorted slot that no longer fits the segment
       const uint32_t r0 = lane * 2, r1 = lane * 2 + 1;
       const uint32_t c0 = s_cur[r0], c1 = s_cur[r1];
       const uint32_t pair = c0 + c1;
@@ -155,12 +166,16 @@ static __global__ void __launch_bounds__(kPartThreads, 8) part_scatter_kernel(co
         if (lane >= static_cast<uint32_t>(d)) incl += x;
       }
       const uint32_t b0 = incl - pair;
-      s_lbase[r0] = b0;
-      s_lbase[r1] = b0 + c0;
-      s_cur[r0] = b0;
-      s_cur[r1] = b0 + c0;
-      s_gbase[r0] = c0 ? atomicAdd(&a.hdr->fill[r0], c0) : 0u;
-      s_gbase[r1] = c1 ? atomicAdd(&a.hdr->fill[r1], c1) : 0u;
+#pragma unroll
+      for (int h = 0; h < 2; h++) {
+        const uint32_t r = h ? r1 : r0, c = h ? c1 : c0, lb = h ? b0 + c0 : b0;
+        const uint32_t g = c ? atomicAdd(&a.hdr->fill[r], c) : 0u;
+        const uint64_t cap = r + 1 < a.n_ranges ? a.seg_cap : a.last_cap;
+        const uint64_t room = g < cap ? cap - g : 0;
+        s_cur[r] = lb;
+        s_lim[r] = lb + static_cast<uint32_t>(room < c ? room : c);
+        s_dst[r] = static_cast<uint64_t>(r) * a.seg_cap + g - lb;
+      }
       if (lane == 31) s_valid = incl;
     }
     __syncthreads();
@@ -172,7 +187,7 @@ static __global__ void __launch_bounds__(kPartThreads, 8) part_scatter_kernel(co
 #pragma unroll
       for (int q = 0; q < 4; q++) {
         if (li + q >= lo && li + q < hi) {
-          const uint32_t slot = atomicAdd(&s_cur[key_range(k[q], a)], 1u);
+          const uint32_t slot = atomicAdd(&s_cur[(rr[i] >> (8 * q)) & 0xffu], 1u);
           s_keys[slot] = k[q];
           s_idx[slot] = static_cast<uint16_t>(li + q);
         }
@@ -184,11 +199,9 @@ static __global__ void __launch_bounds__(kPartThreads, 8) part_scatter_kernel(co
     for (uint32_t sl = threadIdx.x; sl < nv; sl += blockDim.x) {
       const uint32_t key = s_keys[sl];
       const uint32_t r = key_range(key, a);
-      const uint32_t g = s_gbase[r] + (sl - s_lbase[r]);
-      const uint64_t cap = r + 1 < a.n_ranges ? a.seg_cap : a.last_cap;
       const uint2 pr = make_uint2(key, pos0 + s_idx[sl]);
-      if (g < cap) {
-        __stcs(a.pairs + static_cast<uint64_t>(r) * a.seg_cap + g, pr);
+      if (sl < s_lim[r]) {
+        __stcs(a.pairs + (s_dst[r] + sl), pr);
       } else {
         atomicOr(&s_over, 1ull << r);
         if (a.spill) a.spill[atomicAdd(&a.hdr->spill_cnt, 1u)] = pr;

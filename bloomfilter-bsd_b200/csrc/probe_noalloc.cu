@@ -117,6 +117,9 @@ extern "C" dtlg_status dtlg_batch_contains_noalloc(const dtlg_filter* f, const u
   a.err = &h->err;
   a.n_tiles = tiles;
   set_filter_args(f->d, &a);
+  // 256-bit block loads where the words are 32-byte aligned (as every plan of
+  // dtlg_batch_contains_async reads them)
+  a.vec32 = (reinterpret_cast<uintptr_t>(filter_words) & 31u) == 0 ? 1u : 0u;
   const probe_fn fn = f->pk->probe;
   const occ_fn occ = f->pk->probe_blocks_per_sm;
   const int per_sm = std::max(1, occ());
