@@ -390,6 +390,24 @@ class RefProbe:
                 f"the reference's batch_contains ({self.variant}{u})")
 
 
+def spread_copy(a, threads):
+    """A copy of `a` whose pages are first touched by `threads` threads, one
+    contiguous slice each: on a host with several memory nodes the pages land
+    spread over them, as those of a filter and key set that many threads built
+    (an array copied from the GPU by one thread sits on one node, and the
+    probes of every thread on another node then read remote memory)."""
+    import numpy as np
+    from concurrent.futures import ThreadPoolExecutor
+    out = np.empty_like(a)
+    step = -(-len(a) // max(1, threads))
+
+    def part(i):
+        out[i:i + step] = a[i:i + step]
+    with ThreadPoolExecutor(max(1, threads)) as ex:
+        list(ex.map(part, range(0, len(a), step)))
+    return out
+
+
 def list_checksum(pos):
     """Order-sensitive checksum of a position list: sum of pos[i] * (2i + 1)
     mod 2^64 (any reordering, loss or change of a position changes it)."""
@@ -612,8 +630,8 @@ def run_dtlg(args):
     if check_parity:
         try:
             threads = len(os.sched_getaffinity(0))
-            words_np = words.cpu().numpy().view(np.uint64)
-            probe_np = keys.cpu().numpy().view(np.uint32)
+            words_np = spread_copy(words.cpu().numpy().view(np.uint64), threads)
+            probe_np = spread_copy(keys.cpu().numpy().view(np.uint32), threads)
             if args.workload in CUCKOO_WORKLOADS:
                 fcfg = ("cuckoo", tag_bits, slots)
             elif args.workload in BCF_WORKLOADS:

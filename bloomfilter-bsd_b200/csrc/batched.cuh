@@ -227,12 +227,19 @@ __device__ __forceinline__ void build_range(const BatchDesc& d, uint32_t rg, uns
   __syncthreads();
   const uint32_t cnt = min(ld_weak_32(d.cursor + rg), d.bucket_cap);
   const uint32_t* bk = d.bucket + static_cast<uint64_t>(rg) * d.bucket_cap;
+  // The range's words sit in shared memory with the word index of local block
+  // b XORed with bits 1.. of b: a 64-byte block spans 16 of the 32 banks, so
+  // word w of random blocks would fall on just 2 (u32 words) or 4 (u64 halves)
+  // banks, and a warp's atomics on the same word of 32 blocks would conflict
+  // 8 to 16 ways; swizzled they spread over 16 or 32 banks.
   for (uint32_t i = threadIdx.x; i < cnt; i += kBatchThreads) {
     const uint32_t key = ld_weak_32(bk + i);
-    Word* base = s_w + static_cast<uint64_t>(block_index(key * mul_const(0), d.addr) - blk0) * kW;
+    const uint32_t lb = block_index(key * mul_const(0), d.addr) - blk0;
+    const uint32_t swz = (lb >> 1) & (kW - 1);
+    Word* base = s_w + static_cast<uint64_t>(lb) * kW;
     static_for<BloomOps<Cfg>::kS.ng>([&](auto G) {
       constexpr int g = decltype(G)::value;
-      Word* p = base + BloomOps<Cfg>::template group_word<g>(key);
+      Word* p = base + (BloomOps<Cfg>::template group_word<g>(key) ^ swz);
       const Word m = BloomOps<Cfg>::template group_mask<g>(key);
       if constexpr (sizeof(Word) == 8) {
         // 32-bit shared-memory atomics on the halves that have bits to set
@@ -248,7 +255,7 @@ __device__ __forceinline__ void build_range(const BatchDesc& d, uint32_t rg, uns
   __syncthreads();
   Word* gw = static_cast<Word*>(d.words) + static_cast<uint64_t>(blk0) * kW;
   for (uint32_t i = threadIdx.x; i < nw; i += kBatchThreads) {
-    const Word v = s_w[i];
+    const Word v = s_w[i ^ ((i / kW >> 1) & (kW - 1))];  // word i % kW of block i / kW, unswizzled
     if (v == 0) continue;
     if constexpr (sizeof(Word) == 8) {
       gw[i] = static_cast<Word>(ld_weak_64(gw + i)) | v;
