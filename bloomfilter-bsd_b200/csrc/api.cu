@@ -312,13 +312,20 @@ cudaError_t launch_partition(const dtlg_filter* f, const uint32_t* keys_al, uint
   pa.tile_overflow = reinterpret_cast<unsigned long long*>(wsb + lay.tflags_off);
   pa.pairs = reinterpret_cast<uint2*>(wsb + lay.pairs_off);
   pa.spill = spill;
-  static const int scatter_occ = [] {
+  auto occupancy = [](void (*k)(PartArgs)) {
     int o = 0;
-    return cudaOccupancyMaxActiveBlocksPerMultiprocessor(&o, part_scatter_kernel, kPartThreads, 0) == cudaSuccess
-               ? std::max(1, o) : 1;
-  }();
-  const int sgrid = static_cast<int>(std::min<uint64_t>(pa.n_tiles, static_cast<uint64_t>(sms) * scatter_occ));
-  part_scatter_kernel<<<sgrid, kPartThreads, 0, stream>>>(pa);
+    return cudaOccupancyMaxActiveBlocksPerMultiprocessor(&o, k, kPartThreads, 0) == cudaSuccess ? std::max(1, o) : 1;
+  };
+  static const int occ_pow2 = occupancy(part_scatter_kernel<false>);
+  static const int occ_magic = occupancy(part_scatter_kernel<true>);
+  const bool magic = pa.addr.magic_mode != 0;
+  const int sgrid = static_cast<int>(
+      std::min<uint64_t>(pa.n_tiles, static_cast<uint64_t>(sms) * (magic ? occ_magic : occ_pow2)));
+  if (magic) {
+    part_scatter_kernel<true><<<sgrid, kPartThreads, 0, stream>>>(pa);
+  } else {
+    part_scatter_kernel<false><<<sgrid, kPartThreads, 0, stream>>>(pa);
+  }
   *out = pa;
   return cudaGetLastError();
 }

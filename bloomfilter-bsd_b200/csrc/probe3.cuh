@@ -41,9 +41,8 @@
 
 namespace dtlg {
 
-constexpr int kPartThreads = 256;
-constexpr int kPartKeysPerThread = 16;                  // 4 key vectors
-constexpr uint32_t kPartTile = kPartThreads * kPartKeysPerThread;  // 4096 keys
+constexpr uint32_t kPartTile = 4096;                    // keys per scatter tile
+constexpr int kPartThreads = 512;                       // scatter CTA: 8 keys (2 key vectors) per thread
 constexpr int kMaxRanges = 64;
 constexpr uint32_t kPartChunk = 2048;                   // pairs per chunk of a segment
 constexpr uint32_t kPartHeaderBytes = 512;              // fill counters + overflow counters
@@ -100,117 +99,148 @@ __device__ __forceinline__ uint32_t key_range(uint32_t key, const PartArgs& a) {
   return block_index(key * a.block_mul, a.addr) >> a.range_log2;
 }
 
+// key_range with the addressing mode fixed at compile time (block_index
+// branches on it at run time).
+template <bool MAGIC>
+__device__ __forceinline__ uint32_t key_range_of(uint32_t key, const PartArgs& a) {
+  const uint32_t h = key * a.block_mul;
+  uint32_t b;
+  if (MAGIC) {
+    const uint32_t q = __umulhi(h, a.addr.magic) >> a.addr.shift;
+    b = h - q * a.addr.divisor;
+  } else {
+    b = __umulhi(h, a.addr.pow2_mul);
+  }
+  return b >> a.range_log2;
+}
+
+// Shared memory of one scatter CTA.
+struct ScatterSmem {
+  uint32_t keys[kPartTile];            // the tile's keys sorted by range
+  uint16_t idx[kPartTile];             // their tile-local indexes
+  uint32_t cur[kMaxRanges];            // counts, then the placement cursor
+  uint32_t lim[kMaxRanges];            // sorted slots below this go to the segment, the rest overflow
+  unsigned long long dst[kMaxRanges];  // pair index of sorted slot 0 for the range's run
+  uint32_t valid;
+  unsigned long long over;
+};
+
 // One pass: per tile, count the keys of every range, reserve the tile's run of
 // each range in its segment (one global atomic per tile and range), sort the
 // tile by range in shared memory and write every run with consecutive
 // addresses.  Shared memory holds the sorted keys and their 12-bit tile
-// positions (24 KiB), so eight CTAs fit on an SM.  The kernel is bound by
-// instruction issue, so the tile's index arithmetic is 32-bit, a key's range
-// is computed once for the count and the placement (kept as bytes), and each
-// range's destination base and slot limit are computed once per tile.
-static __global__ void __launch_bounds__(kPartThreads, 8) part_scatter_kernel(const __grid_constant__ PartArgs a) {
-  __shared__ uint32_t s_keys[kPartTile];
-  __shared__ uint16_t s_idx[kPartTile];
-  __shared__ uint32_t s_cur[kMaxRanges];    // counts, then the placement cursor
-  __shared__ uint32_t s_lim[kMaxRanges];    // sorted slots below this go to the segment, the rest overflow
-  __shared__ unsigned long long s_dst[kMaxRanges];  // pair index of sorted slot 0 for the range's run
-  __shared__ uint32_t s_valid;
-  __shared__ unsigned long long s_over;
-  const uint4* keys4 = reinterpret_cast<const uint4*>(a.keys_al);
+// positions (24 KiB).  The kernel is bound by instruction issue, so the
+// addressing mode is a template parameter (POW2 or MAGIC, chosen by the
+// launch), the tile's index arithmetic is 32-bit, a key's range is computed
+// once for the count and the placement (kept as bytes), and each range's
+// destination base and slot limit are computed once per tile.  512 threads of
+// 8 keys each, four CTAs per SM (2^28 keys over 64 ranges of a 512 MiB POW2
+// filter: 959 us with 256 threads of 16 keys and run-time addressing, 896 us
+// so).
+template <bool MAGIC, int THREADS>
+__device__ __forceinline__ void scatter_tile(const PartArgs& a, uint32_t tile, ScatterSmem& S) {
+  constexpr int kVecs = static_cast<int>(kPartTile) / THREADS / 4;  // key vectors per thread
+  static_assert(kVecs * 4 * THREADS == static_cast<int>(kPartTile), "tile");
   const uint32_t lane = threadIdx.x & 31u;
-  for (uint32_t tile = blockIdx.x; tile < a.n_tiles; tile += gridDim.x) {
-    if (threadIdx.x < kMaxRanges) s_cur[threadIdx.x] = 0;
-    if (threadIdx.x == 0) s_over = 0;
-    __syncthreads();
-    const uint64_t tile_pos = static_cast<uint64_t>(tile) * kPartTile;  // physical index of the tile's key 0
-    // valid keys of this tile: tile-local indexes [lo, hi)
-    const uint32_t lo = tile_pos < a.pre ? static_cast<uint32_t>(a.pre - tile_pos) : 0u;
-    const uint32_t hi = a.n_phys - tile_pos < kPartTile ? static_cast<uint32_t>(a.n_phys - tile_pos) : kPartTile;
-    const uint4* t4 = keys4 + tile_pos / 4;
-    // the keys are read twice: for the counts and, from L2, for the placement
-    // (holding them across the scan would not fit 32 registers); their ranges
-    // are kept, four bytes per register
-    uint32_t rr[kPartKeysPerThread / 4];
-    {
-      uint4 kv[kPartKeysPerThread / 4];
+  const uint64_t tile_pos = static_cast<uint64_t>(tile) * kPartTile;  // physical index of the tile's key 0
+  // valid keys of this tile: tile-local indexes [lo, hi)
+  const uint32_t lo = tile_pos < a.pre ? static_cast<uint32_t>(a.pre - tile_pos) : 0u;
+  const uint32_t hi = a.n_phys - tile_pos < kPartTile ? static_cast<uint32_t>(a.n_phys - tile_pos) : kPartTile;
+  const uint4* t4 = reinterpret_cast<const uint4*>(a.keys_al) + tile_pos / 4;
+  // the keys are read twice: for the counts and, from L2, for the placement
+  // (holding them across the scan would not fit 32 registers); their ranges
+  // are kept, four bytes per register
+  uint32_t rr[kVecs];
+  {
+    uint4 kv[kVecs];
 #pragma unroll
-      for (int i = 0; i < kPartKeysPerThread / 4; i++) {
-        const uint32_t li = (i * kPartThreads + threadIdx.x) * 4;
-        kv[i] = li < hi ? __ldcg(t4 + li / 4) : make_uint4(0, 0, 0, 0);
-      }
-#pragma unroll
-      for (int i = 0; i < kPartKeysPerThread / 4; i++) {
-        const uint32_t li = (i * kPartThreads + threadIdx.x) * 4;
-        const uint32_t k[4] = {kv[i].x, kv[i].y, kv[i].z, kv[i].w};
-        rr[i] = 0;
-#pragma unroll
-        for (int q = 0; q < 4; q++) {
-          const uint32_t r = key_range(k[q], a);
-          rr[i] |= r << (8 * q);
-          if (li + q >= lo && li + q < hi) atomicAdd(&s_cur[r], 1u);
-        }
-      }
+    for (int i = 0; i < kVecs; i++) {
+      const uint32_t li = (i * THREADS + threadIdx.x) * 4;
+      kv[i] = li < hi ? __ldcg(t4 + li / 4) : make_uint4(0, 0, 0, 0);
     }
-    __syncthreads();
-    if (threadIdx.x < 32) {
-      // tile-local run starts (exclusive scan, two ranges per lane), the runs'
-      // slots in their segments, and per range the destination of sorted slot
-      // 0 and the first sorted slot that no longer fits the segment
-      const uint32_t r0 = lane * 2, r1 = lane * 2 + 1;
-      const uint32_t c0 = s_cur[r0], c1 = s_cur[r1];
-      const uint32_t pair = c0 + c1;
-      uint32_t incl = pair;
 #pragma unroll
-      for (int d = 1; d < 32; d <<= 1) {
-        const uint32_t x = __shfl_up_sync(0xffffffffu, incl, d);
-        if (lane >= static_cast<uint32_t>(d)) incl += x;
-      }
-      const uint32_t b0 = incl - pair;
-#pragma unroll
-      for (int h = 0; h < 2; h++) {
-        const uint32_t r = h ? r1 : r0, c = h ? c1 : c0, lb = h ? b0 + c0 : b0;
-        const uint32_t g = c ? atomicAdd(&a.hdr->fill[r], c) : 0u;
-        const uint64_t cap = r + 1 < a.n_ranges ? a.seg_cap : a.last_cap;
-        const uint64_t room = g < cap ? cap - g : 0;
-        s_cur[r] = lb;
-        s_lim[r] = lb + static_cast<uint32_t>(room < c ? room : c);
-        s_dst[r] = static_cast<uint64_t>(r) * a.seg_cap + g - lb;
-      }
-      if (lane == 31) s_valid = incl;
-    }
-    __syncthreads();
-#pragma unroll
-    for (int i = 0; i < kPartKeysPerThread / 4; i++) {
-      const uint32_t li = (i * kPartThreads + threadIdx.x) * 4;
-      const uint4 x = li < hi ? __ldcs(t4 + li / 4) : make_uint4(0, 0, 0, 0);
-      const uint32_t k[4] = {x.x, x.y, x.z, x.w};
+    for (int i = 0; i < kVecs; i++) {
+      const uint32_t li = (i * THREADS + threadIdx.x) * 4;
+      const uint32_t k[4] = {kv[i].x, kv[i].y, kv[i].z, kv[i].w};
+      rr[i] = 0;
 #pragma unroll
       for (int q = 0; q < 4; q++) {
-        if (li + q >= lo && li + q < hi) {
-          const uint32_t slot = atomicAdd(&s_cur[(rr[i] >> (8 * q)) & 0xffu], 1u);
-          s_keys[slot] = k[q];
-          s_idx[slot] = static_cast<uint16_t>(li + q);
-        }
+        const uint32_t r = key_range_of<MAGIC>(k[q], a);
+        rr[i] |= r << (8 * q);
+        if (li + q >= lo && li + q < hi) atomicAdd(&S.cur[r], 1u);
       }
     }
-    __syncthreads();
-    const uint32_t nv = s_valid;
-    const uint32_t pos0 = static_cast<uint32_t>(tile_pos - a.pre);  // logical position of tile index 0 (mod 2^32)
-    for (uint32_t sl = threadIdx.x; sl < nv; sl += blockDim.x) {
-      const uint32_t key = s_keys[sl];
-      const uint32_t r = key_range(key, a);
-      const uint2 pr = make_uint2(key, pos0 + s_idx[sl]);
-      if (sl < s_lim[r]) {
-        __stcs(a.pairs + (s_dst[r] + sl), pr);
-      } else {
-        atomicOr(&s_over, 1ull << r);
-        if (a.spill) a.spill[atomicAdd(&a.hdr->spill_cnt, 1u)] = pr;
+  }
+  __syncthreads();
+  if (threadIdx.x < 32) {
+    // tile-local run starts (exclusive scan, two ranges per lane), the runs'
+    // slots in their segments, and per range the destination of sorted slot
+    // 0 and the first sorted slot that no longer fits the segment
+    const uint32_t r0 = lane * 2, r1 = lane * 2 + 1;
+    const uint32_t c0 = S.cur[r0], c1 = S.cur[r1];
+    const uint32_t pair = c0 + c1;
+    uint32_t incl = pair;
+#pragma unroll
+    for (int d = 1; d < 32; d <<= 1) {
+      const uint32_t x = __shfl_up_sync(0xffffffffu, incl, d);
+      if (lane >= static_cast<uint32_t>(d)) incl += x;
+    }
+    const uint32_t b0 = incl - pair;
+#pragma unroll
+    for (int h = 0; h < 2; h++) {
+      const uint32_t r = h ? r1 : r0, c = h ? c1 : c0, lb = h ? b0 + c0 : b0;
+      const uint32_t g = c ? atomicAdd(&a.hdr->fill[r], c) : 0u;
+      const uint64_t cap = r + 1 < a.n_ranges ? a.seg_cap : a.last_cap;
+      const uint64_t room = g < cap ? cap - g : 0;
+      S.cur[r] = lb;
+      S.lim[r] = lb + static_cast<uint32_t>(room < c ? room : c);
+      S.dst[r] = static_cast<uint64_t>(r) * a.seg_cap + g - lb;
+    }
+    if (lane == 31) S.valid = incl;
+  }
+  __syncthreads();
+#pragma unroll
+  for (int i = 0; i < kVecs; i++) {
+    const uint32_t li = (i * THREADS + threadIdx.x) * 4;
+    const uint4 x = li < hi ? __ldcs(t4 + li / 4) : make_uint4(0, 0, 0, 0);
+    const uint32_t k[4] = {x.x, x.y, x.z, x.w};
+#pragma unroll
+    for (int q = 0; q < 4; q++) {
+      if (li + q >= lo && li + q < hi) {
+        const uint32_t slot = atomicAdd(&S.cur[(rr[i] >> (8 * q)) & 0xffu], 1u);
+        S.keys[slot] = k[q];
+        S.idx[slot] = static_cast<uint16_t>(li + q);
       }
     }
+  }
+  __syncthreads();
+  const uint32_t nv = S.valid;
+  const uint32_t pos0 = static_cast<uint32_t>(tile_pos - a.pre);  // logical position of tile index 0 (mod 2^32)
+  for (uint32_t sl = threadIdx.x; sl < nv; sl += THREADS) {
+    const uint32_t key = S.keys[sl];
+    const uint32_t r = key_range_of<MAGIC>(key, a);
+    const uint2 pr = make_uint2(key, pos0 + S.idx[sl]);
+    if (sl < S.lim[r]) {
+      __stcs(a.pairs + (S.dst[r] + sl), pr);
+    } else {
+      atomicOr(&S.over, 1ull << r);
+      if (a.spill) a.spill[atomicAdd(&a.hdr->spill_cnt, 1u)] = pr;
+    }
+  }
+  __syncthreads();
+}
+
+template <bool MAGIC, int THREADS = kPartThreads>
+static __global__ void __launch_bounds__(THREADS, 2048 / THREADS) part_scatter_kernel(const __grid_constant__ PartArgs a) {
+  __shared__ ScatterSmem S;
+  for (uint32_t tile = blockIdx.x; tile < a.n_tiles; tile += gridDim.x) {
+    if (threadIdx.x < kMaxRanges) S.cur[threadIdx.x] = 0;
+    if (threadIdx.x == 0) S.over = 0;
     __syncthreads();
+    scatter_tile<MAGIC, THREADS>(a, tile, S);
     if (threadIdx.x == 0) {
-      a.tile_overflow[tile] = s_over;
-      if (s_over) atomicAdd(&a.hdr->overflow_tiles, 1u);
+      a.tile_overflow[tile] = S.over;
+      if (S.over) atomicAdd(&a.hdr->overflow_tiles, 1u);
     }
   }
 }

@@ -397,6 +397,16 @@ dtlg_status dtlg_or_words(uint64_t* dst, const uint64_t* src, uint64_t n_words, 
 dtlg_status dtlg_copy_words_peer(uint64_t* dst, int dst_device, const uint64_t* src, int src_device,
                                  uint64_t n_words, dtlg_stream_t stream);
 
+/* ---- the L2 gather roofline (measurement; no reference counterpart) ----
+ * Gathers n_sectors random 32-byte sectors of buf[0, bytes) (a device
+ * pointer, 32-byte aligned) with the probe kernels' 256-bit read-only load
+ * and XORs every word into *sink_dev (mixed, so the loads cannot be dropped).
+ * Sector i is row ((h(i) mod 2^32) * (bytes / 32)) >> 32 of the buffer, h a
+ * 64-bit multiply-xorshift hash of i + 1.  Timed over a buffer the size of an
+ * L2-resident filter, it gives the rate that bounds that filter's probe. */
+dtlg_status dtlg_sector_gather(const uint64_t* buf, uint64_t bytes, uint64_t n_sectors, uint64_t* sink_dev,
+                               dtlg_stream_t stream);
+
 /* ---- single keys: filter_base::insert / contains (filter_base.hpp:22,32) ---- */
 dtlg_status dtlg_insert(const dtlg_filter* f, uint64_t* filter_words, uint32_t key, dtlg_stream_t stream);
 dtlg_status dtlg_contains(const dtlg_filter* f, const uint64_t* filter_words, uint32_t key,
