@@ -107,12 +107,14 @@ __device__ __forceinline__ unsigned int ld_acquire_u32(const unsigned int* p) {
   return v;
 }
 
-// Thread 0 waits (bounded) until *ctr >= need; the CTA then proceeds.
-__device__ __forceinline__ void wait_counter(const unsigned int* ctr, uint32_t need, unsigned int* err) {
+// Thread 0 waits (bounded) until *ctr >= need; the CTA then proceeds.  A wait
+// that spins `limit` times sets bit 1 of *err and gives up.
+__device__ __forceinline__ void wait_counter(const unsigned int* ctr, uint32_t need, unsigned int* err,
+                                             uint32_t limit = kSpinLimit) {
   if (threadIdx.x == 0) {
     uint32_t spins = 0;
     while (ld_acquire_u32(ctr) < need) {
-      if (++spins > kSpinLimit) {
+      if (++spins > limit) {
         atomicOr(err, 2u);
         break;
       }
@@ -232,35 +234,59 @@ __device__ __forceinline__ void build_range(const BatchDesc& d, uint32_t rg, uns
   // word w of random blocks would fall on just 2 (u32 words) or 4 (u64 halves)
   // banks, and a warp's atomics on the same word of 32 blocks would conflict
   // 8 to 16 ways; swizzled they spread over 16 or 32 banks.
-  for (uint32_t i = threadIdx.x; i < cnt; i += kBatchThreads) {
-    const uint32_t key = ld_weak_32(bk + i);
-    const uint32_t lb = block_index(key * mul_const(0), d.addr) - blk0;
-    const uint32_t swz = (lb >> 1) & (kW - 1);
-    Word* base = s_w + static_cast<uint64_t>(lb) * kW;
-    static_for<BloomOps<Cfg>::kS.ng>([&](auto G) {
-      constexpr int g = decltype(G)::value;
-      Word* p = base + (BloomOps<Cfg>::template group_word<g>(key) ^ swz);
-      const Word m = BloomOps<Cfg>::template group_mask<g>(key);
-      if constexpr (sizeof(Word) == 8) {
-        // 32-bit shared-memory atomics on the halves that have bits to set
-        uint32_t* p32 = reinterpret_cast<uint32_t*>(p);
-        const uint32_t lo = static_cast<uint32_t>(m), hi = static_cast<uint32_t>(m >> 32);
-        if (lo) atomicOr(p32, lo);
-        if (hi) atomicOr(p32 + 1, hi);
-      } else {
-        atomicOr(reinterpret_cast<uint32_t*>(p), static_cast<uint32_t>(m));
-      }
-    });
+  // kU bucket keys per thread in flight: each load comes from L2 or DRAM, and
+  // one at a time left the loop waiting on it (long scoreboard)
+  constexpr int kU = 4;
+  for (uint32_t i0 = 0; i0 < cnt; i0 += kBatchThreads * kU) {
+    uint32_t kk[kU];
+#pragma unroll
+    for (int u = 0; u < kU; u++) {
+      const uint32_t i = i0 + u * kBatchThreads + threadIdx.x;
+      kk[u] = i < cnt ? ld_weak_32(bk + i) : 0u;
+    }
+#pragma unroll
+    for (int u = 0; u < kU; u++) {
+      if (i0 + u * kBatchThreads + threadIdx.x >= cnt) break;
+      const uint32_t key = kk[u];
+      const uint32_t lb = block_index(key * mul_const(0), d.addr) - blk0;
+      const uint32_t swz = (lb >> 1) & (kW - 1);
+      Word* base = s_w + static_cast<uint64_t>(lb) * kW;
+      static_for<BloomOps<Cfg>::kS.ng>([&](auto G) {
+        constexpr int g = decltype(G)::value;
+        Word* p = base + (BloomOps<Cfg>::template group_word<g>(key) ^ swz);
+        const Word m = BloomOps<Cfg>::template group_mask<g>(key);
+        if constexpr (sizeof(Word) == 8) {
+          // 32-bit shared-memory atomics on the halves that have bits to set
+          uint32_t* p32 = reinterpret_cast<uint32_t*>(p);
+          const uint32_t lo = static_cast<uint32_t>(m), hi = static_cast<uint32_t>(m >> 32);
+          if (lo) atomicOr(p32, lo);
+          if (hi) atomicOr(p32 + 1, hi);
+        } else {
+          atomicOr(reinterpret_cast<uint32_t*>(p), static_cast<uint32_t>(m));
+        }
+      });
+    }
   }
   __syncthreads();
   Word* gw = static_cast<Word*>(d.words) + static_cast<uint64_t>(blk0) * kW;
-  for (uint32_t i = threadIdx.x; i < nw; i += kBatchThreads) {
-    const Word v = s_w[i ^ ((i / kW >> 1) & (kW - 1))];  // word i % kW of block i / kW, unswizzled
-    if (v == 0) continue;
-    if constexpr (sizeof(Word) == 8) {
-      gw[i] = static_cast<Word>(ld_weak_64(gw + i)) | v;
-    } else {
-      gw[i] = static_cast<Word>(ld_weak_32(gw + i)) | v;
+  for (uint32_t i0 = 0; i0 < nw; i0 += kBatchThreads * kU) {
+    Word v[kU], w[kU];
+#pragma unroll
+    for (int u = 0; u < kU; u++) {
+      const uint32_t i = i0 + u * kBatchThreads + threadIdx.x;
+      v[u] = i < nw ? s_w[i ^ ((i / kW >> 1) & (kW - 1))] : Word(0);  // word i % kW of block i / kW, unswizzled
+      w[u] = 0;
+      if (v[u] != 0) {
+        if constexpr (sizeof(Word) == 8) {
+          w[u] = static_cast<Word>(ld_weak_64(gw + i));
+        } else {
+          w[u] = static_cast<Word>(ld_weak_32(gw + i));
+        }
+      }
+    }
+#pragma unroll
+    for (int u = 0; u < kU; u++) {
+      if (v[u] != 0) gw[i0 + u * kBatchThreads + threadIdx.x] = w[u] | v[u];
     }
   }
 }
@@ -305,16 +331,30 @@ __global__ void __launch_bounds__(kBatchThreads, 4) batched_kernel(const __grid_
           scatter_tile<Cfg>(d, k0, s_dyn, s_wtot);
           return;
         }
+        using Ops = BloomOps<Cfg>;
         const uint4* k4 = reinterpret_cast<const uint4*>(d.build_keys + k0);
+        if constexpr (Ops::kLaneInsert && sizeof(typename Ops::LaneStage) * (kBatchThreads / 32) <= kBatchRangeBytes) {
+          // warp-cooperative inserts (BloomOps::insert_lanes), staged in s_dyn
+          typename Ops::LaneStage& my = reinterpret_cast<typename Ops::LaneStage*>(s_dyn)[threadIdx.x >> 5];
 #pragma unroll
-        for (int r = 0; r < kRounds; r++) {
-          const uint64_t i0 = static_cast<uint64_t>(r) * (kBatchThreads * 4) + threadIdx.x * 4u;
-          if (k0 + i0 >= d.n_build) continue;
-          const uint4 kv = __ldcs(k4 + (i0 >> 2));
-          const uint32_t k[4] = {kv.x, kv.y, kv.z, kv.w};
+          for (int r = 0; r < kRounds; r++) {
+            const uint64_t i0 = static_cast<uint64_t>(r) * (kBatchThreads * 4) + threadIdx.x * 4u;
+            const uint4 kv = k0 + i0 < d.n_build ? __ldcs(k4 + (i0 >> 2)) : make_uint4(0, 0, 0, 0);
+            const uint32_t k[4] = {kv.x, kv.y, kv.z, kv.w};
 #pragma unroll
-          for (int q = 0; q < 4; q++)
-            if (k0 + i0 + q < d.n_build) BloomOps<Cfg>::insert(d.words, k[q], d.addr);
+            for (int q = 0; q < 4; q++) Ops::insert_lanes(d.words, k[q], k0 + i0 + q < d.n_build, d.addr, my);
+          }
+        } else {
+#pragma unroll
+          for (int r = 0; r < kRounds; r++) {
+            const uint64_t i0 = static_cast<uint64_t>(r) * (kBatchThreads * 4) + threadIdx.x * 4u;
+            if (k0 + i0 >= d.n_build) continue;
+            const uint4 kv = __ldcs(k4 + (i0 >> 2));
+            const uint32_t k[4] = {kv.x, kv.y, kv.z, kv.w};
+#pragma unroll
+            for (int q = 0; q < 4; q++)
+              if (k0 + i0 + q < d.n_build) Ops::insert(d.words, k[q], d.addr);
+          }
         }
       });
       __syncthreads();

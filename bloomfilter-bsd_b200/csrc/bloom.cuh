@@ -319,23 +319,86 @@ struct BloomOps {
       atomic_or_word<Word>(base + group_word<g>(key), group_mask<g>(key));
     });
   }
+
+  // Warp-cooperative insert.  Every lane brings one key (valid or not); the
+  // kS.ng word updates of each key are spread over kS.ng lanes, so one warp
+  // instruction carries the updates of 32 / kS.ng whole keys and those of one
+  // key reach the L2 in one request per 32-byte sector, where they are applied
+  // together.  One thread per key issues its kS.ng atomic ORs one after the
+  // other, each a request of its own: on B200, 64-byte blocks of 8 u64 words
+  // with one bit each, 2^26 keys into 8 MiB build at 82.6 Gkeys/s this way
+  // against 23.6 (and into 512 MiB at 24.5 against 6.7).  All 32 lanes call it.
+  static constexpr bool kLaneInsert = kS.ng >= 2 && kS.ng <= 32 && (32 % kS.ng) == 0;
+  struct LaneStage {            // per warp, in shared memory
+    Word mask[32 * kS.ng];      // [key lane][group]
+    uint8_t word[32 * kS.ng];   // word of the group in its block (hashed layouts)
+    uint32_t blk[32];           // block of each lane's key
+  };
+  __device__ __forceinline__ static void insert_lanes(void* filter, uint32_t key, bool valid, const Addr& a,
+                                                      LaneStage& st) {
+    static_assert(kLaneInsert, "groups per key must divide the warp");
+    constexpr int kNg = kS.ng;
+    const uint32_t lane = threadIdx.x & 31u;
+    st.blk[lane] = block_index(key * mul_const(0), a);
+    static_for<kNg>([&](auto G) {
+      constexpr int g = decltype(G)::value;
+      st.mask[lane * kNg + g] = valid ? group_mask<g>(key) : Word(0);
+      if constexpr (!kS.fixed_words) st.word[lane * kNg + g] = static_cast<uint8_t>(group_word<g>(key));
+    });
+    // with fixed words, this lane's group (lane % kNg) always has the same word
+    uint32_t wl = 0;
+    if constexpr (kS.fixed_words) {
+      static_for<kNg>([&](auto G) {
+        constexpr int g = decltype(G)::value;
+        if (lane % kNg == g) wl = kS.g[g].wconst;
+      });
+    }
+    __syncwarp();
+#pragma unroll
+    for (int j = 0; j < kNg; j++) {
+      const uint32_t i = j * 32 + lane;  // group i % kNg of the key of lane i / kNg
+      const Word m = st.mask[i];
+      const uint32_t w = kS.fixed_words ? wl : st.word[i];
+      if (m) atomic_or_word<Word>(static_cast<Word*>(filter) + static_cast<uint64_t>(st.blk[i / kNg]) * kW + w, m);
+    }
+    __syncwarp();
+  }
 };
 
 // batch_insert (blocked_bloomfilter_logic.hpp:111-117).  The reference inserts
 // sequentially with a CAS-OR per word (..._sgew.hpp:300-325); OR commutes, so
 // concurrent atomic ORs give the same words in any order.
+// Layouts with 2..32 word groups per key insert warp-cooperatively
+// (BloomOps::insert_lanes); the loop then runs warp-uniformly.
 template <class Cfg>
 __global__ void __launch_bounds__(256) bloom_build_kernel(const __grid_constant__ BuildArgs a) {
+  using Ops = BloomOps<Cfg>;
   const uint4* keys4 = reinterpret_cast<const uint4*>(a.keys_al);
   const uint64_t nvec = (a.n_phys + 3) >> 2;
-  for (uint64_t v = blockIdx.x * static_cast<uint64_t>(blockDim.x) + threadIdx.x; v < nvec;
-       v += static_cast<uint64_t>(gridDim.x) * blockDim.x) {
-    const uint4 kv = __ldcs(keys4 + v);
-    const uint32_t k[4] = {kv.x, kv.y, kv.z, kv.w};
+  const uint64_t stride = static_cast<uint64_t>(gridDim.x) * blockDim.x;
+  if constexpr (Ops::kLaneInsert) {
+    __shared__ typename Ops::LaneStage st[8];
+    typename Ops::LaneStage& my = st[threadIdx.x >> 5];
+    for (uint64_t vb = blockIdx.x * static_cast<uint64_t>(blockDim.x) + (threadIdx.x & ~31u); vb < nvec;
+         vb += stride) {
+      const uint64_t v = vb + (threadIdx.x & 31u);
+      const uint4 kv = v < nvec ? __ldcs(keys4 + v) : make_uint4(0, 0, 0, 0);
+      const uint32_t k[4] = {kv.x, kv.y, kv.z, kv.w};
 #pragma unroll
-    for (int q = 0; q < 4; q++) {
-      const uint64_t p = v * 4 + q;
-      if (p >= a.pre && p < a.n_phys) BloomOps<Cfg>::insert(a.filter, k[q], a.addr);
+      for (int q = 0; q < 4; q++) {
+        const uint64_t p = v * 4 + q;
+        Ops::insert_lanes(a.filter, k[q], p >= a.pre && p < a.n_phys, a.addr, my);
+      }
+    }
+  } else {
+    for (uint64_t v = blockIdx.x * static_cast<uint64_t>(blockDim.x) + threadIdx.x; v < nvec; v += stride) {
+      const uint4 kv = __ldcs(keys4 + v);
+      const uint32_t k[4] = {kv.x, kv.y, kv.z, kv.w};
+#pragma unroll
+      for (int q = 0; q < 4; q++) {
+        const uint64_t p = v * 4 + q;
+        if (p >= a.pre && p < a.n_phys) Ops::insert(a.filter, k[q], a.addr);
+      }
     }
   }
 }
@@ -348,8 +411,15 @@ __global__ void __launch_bounds__(256) bloom_build_kernel(const __grid_constant_
 template <class Cfg>
 __global__ void __launch_bounds__(256) bloom_build_pairs_kernel(const __grid_constant__ PartArgs pa, void* filter,
                                                                 const Addr addr) {
-  auto ins = [&](uint32_t key, uint32_t) { BloomOps<Cfg>::insert(filter, key, addr); };
-  for_each_pair(seg_chunks(pa), ins);
+  using Ops = BloomOps<Cfg>;
+  auto ins = [&](uint32_t key, uint32_t) { Ops::insert(filter, key, addr); };
+  if constexpr (Ops::kLaneInsert) {
+    __shared__ typename Ops::LaneStage st[8];
+    typename Ops::LaneStage& my = st[threadIdx.x >> 5];
+    for_each_pair_warp(seg_chunks(pa), [&](uint32_t key, bool valid) { Ops::insert_lanes(filter, key, valid, addr, my); });
+  } else {
+    for_each_pair(seg_chunks(pa), ins);
+  }
   for_each_overflow_key(pa, ins);
 }
 

@@ -65,7 +65,9 @@ __device__ __forceinline__ void st_volatile(unsigned long long* p, unsigned long
 }
 
 // Exclusive prefix of this tile from the predecessors' status words (warp 0).
-__device__ __forceinline__ uint32_t look_back(const ProbeArgs& a, uint32_t tile, uint32_t lane) {
+// A wait that spins `limit` times sets bit 0 of *a.err and returns what it has.
+__device__ __forceinline__ uint32_t look_back(const ProbeArgs& a, uint32_t tile, uint32_t lane,
+                                              uint32_t limit = kSpinLimit) {
   uint32_t excl = 0;
   int64_t pred = static_cast<int64_t>(tile) - 1;
   uint32_t spins = 0;
@@ -78,7 +80,7 @@ __device__ __forceinline__ uint32_t look_back(const ProbeArgs& a, uint32_t tile,
     // lanes 0..fp (nearest predecessors first) must all be ready
     const uint32_t need = prefix ? ((prefix & (0u - prefix)) << 1) - 1u : 0xffffffffu;
     if (not_ready & need) {
-      if (++spins > kSpinLimit) {
+      if (++spins > limit) {
         if (lane == 0) atomicOr(a.err, 1u);
         break;
       }

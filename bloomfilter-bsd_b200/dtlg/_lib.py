@@ -135,6 +135,7 @@ SIGNATURES = {
     "dtlg_or_words": (_i, [_vp, _vp, _u64, _u32, _u64, _vp]),
     "dtlg_copy_words_peer": (_i, [_vp, C.c_int, _vp, C.c_int, _u64, _vp]),
     "dtlg_sector_gather": (_i, [_vp, _u64, _u64, _vp, _vp]),
+    "dtlg_check_wait_timeout": (_i, [_u32, C.POINTER(_u32)]),
     "dtlg_insert": (_i, [_vp, _vp, _u32, _vp]),
     "dtlg_contains": (_i, [_vp, _vp, _u32, C.POINTER(_i), _vp]),
     "dtlg_batch_contains_host": (_i, [_vp, _vp, _vp, _u64, _vp, _u32, _u64p, _vp]),

@@ -407,6 +407,17 @@ dtlg_status dtlg_copy_words_peer(uint64_t* dst, int dst_device, const uint64_t* 
 dtlg_status dtlg_sector_gather(const uint64_t* buf, uint64_t bytes, uint64_t n_sectors, uint64_t* sink_dev,
                                dtlg_stream_t stream);
 
+/* ---- failure detection of the device waits (no reference counterpart) ----
+ * The look-back of the ordered compaction and the batched kernel's item
+ * dependencies wait on words written by other CTAs, each wait bounded; one
+ * that runs out sets an error bit and the call reports DTLG_ERR_TIMEOUT.
+ * This runs both wait loops on the current device against words that nothing
+ * ever sets, with `spin_limit` spins (1 .. 2^22; each spin sleeps ~0.1 us),
+ * synchronizes the device and stores the error bits they set in *err_bits:
+ * bit 0 the look-back, bit 1 the dependency wait (3 = both gave up and
+ * reported; the kernel ends either way and the context stays usable). */
+dtlg_status dtlg_check_wait_timeout(uint32_t spin_limit, uint32_t* err_bits);
+
 /* ---- single keys: filter_base::insert / contains (filter_base.hpp:22,32) ---- */
 dtlg_status dtlg_insert(const dtlg_filter* f, uint64_t* filter_words, uint32_t key, dtlg_stream_t stream);
 dtlg_status dtlg_contains(const dtlg_filter* f, const uint64_t* filter_words, uint32_t key,
