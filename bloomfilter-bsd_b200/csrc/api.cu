@@ -465,7 +465,8 @@ dtlg_status launch_probe(const dtlg_filter* f, const uint64_t* words, const uint
 // for n keys: 1 = one kernel of global atomics, 2 = keys grouped by L2-sized
 // block range first (the probe's partition).  Automatic: the partitioned
 // build for Bloom filters beyond 160 MiB and batches of >= 2^20 keys (512 MiB,
-// 2^28 keys: 40.0 -> 19.9 ms).  A blocked cuckoo key takes one or two
+// 2^28 keys: 10.97 -> 6.56 ms; 256 MiB: 4.46 -> 3.31 ms; 64 MiB stays with plan
+// 1, 0.82 against 0.90 ms).  A blocked cuckoo key takes one or two
 // compare-and-swaps, too few to repay the partition (256 MiB, 2^26 keys:
 // 2.60 -> 2.70 ms), so its plan 2 is only taken on request.
 int block_build_plan(const dtlg_filter* f, uint64_t n) {
