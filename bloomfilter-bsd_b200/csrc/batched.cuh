@@ -76,6 +76,10 @@ constexpr uint32_t kItemBuild = 0;   // y: the filter's build tile
 constexpr uint32_t kItemRange = 1;   // y: the range of a staged filter
 constexpr uint32_t kItemProbe = 2;   // y: the global probe tile
 constexpr uint32_t kItemCompact = 3; // y: the global compact tile (look-back word)
+// Probe keys a thread tests together (BloomOps::testn_weak): their first
+// loads are all in flight before any is tested.  512-filter mix, probe phase:
+// 7.15 ms one at a time, 6.62 ms by two; four spill at the 64-register bound.
+constexpr int kTestN = 2;
 constexpr uint32_t kBatchCompactKeys = 65536;  // keys per compact tile: 8 warps x 8 rows x 32 words
 
 struct BatchArgs {
@@ -391,21 +395,25 @@ __global__ void __launch_bounds__(kBatchThreads, 4) batched_kernel(const __grid_
       dispatch_cfg<Cfgs...>(d.cfg, [&](auto c) {
         using Cfg = decltype(c);
         const uint4* k4 = reinterpret_cast<const uint4*>(d.probe_keys + k0);
-#pragma unroll
+#pragma unroll 1
         for (int r = 0; r < kRounds; r++) {
           const uint32_t i0 = r * (kBatchThreads * 4) + threadIdx.x * 4u;
           uint32_t fl = 0;
           if (k0 + i0 < d.n_probe) {
             const uint4 kv = __ldcs(k4 + (i0 >> 2));
             const uint32_t k[4] = {kv.x, kv.y, kv.z, kv.w};
+            const typename Cfg::word_t* base[4];
 #pragma unroll
             for (int q = 0; q < 4; q++) {
               const uint32_t blk = block_index(k[q] * mul_const(0), d.addr);
-              const auto* base = static_cast<const typename Cfg::word_t*>(d.words) +
-                                 static_cast<uint64_t>(blk) * Cfg::kW;
-              const bool hit = BloomOps<Cfg>::template test_block<false>(base, k[q], vec32);
-              fl |= ((hit && k0 + i0 + q < d.n_probe) ? 1u : 0u) << q;
+              base[q] = static_cast<const typename Cfg::word_t*>(d.words) + static_cast<uint64_t>(blk) * Cfg::kW;
             }
+            uint32_t hit = 0;
+#pragma unroll
+            for (int g0 = 0; g0 < 4; g0 += kTestN)
+              hit |= BloomOps<Cfg>::template testn_weak<kTestN>(base + g0, k + g0, vec32) << g0;
+#pragma unroll
+            for (int q = 0; q < 4; q++) fl |= ((((hit >> q) & 1u) && k0 + i0 + q < d.n_probe) ? 1u : 0u) << q;
           }
           // lanes 8j .. 8j+7 hold keys 32j .. 32j+31 of the warp's 128: word j
           uint32_t x = fl << (4u * (lane & 7u));

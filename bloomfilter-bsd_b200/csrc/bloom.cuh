@@ -277,6 +277,79 @@ struct BloomOps {
     return ok;
   }
 
+  // test_block<false> for N keys at once: the N first halves (or first
+  // groups) are loaded before any of them is tested, then the second halves of
+  // the keys that passed, so a thread has N gathers in flight instead of one
+  // (the batched kernel runs at half the SM's warp slots).  Bit q of the
+  // result: key q matches.
+  template <int N>
+  __device__ __forceinline__ static uint32_t testn_weak(const Word* const* base, const uint32_t* key, bool vec32) {
+    uint32_t hit = 0;
+    if constexpr (kHalves) {
+      constexpr int kH = kW / 2;
+      Word v[N][kH];
+#pragma unroll
+      for (int q = 0; q < N; q++) load_block<Word, kH, false>(base[q], v[q], vec32);
+      uint32_t pass = 0;
+#pragma unroll
+      for (int q = 0; q < N; q++) pass |= (test_words<0, kH>(v[q], key[q]) ? 1u : 0u) << q;
+#pragma unroll
+      for (int q = 0; q < N; q++)
+        if ((pass >> q) & 1u) load_block<Word, kH, false>(base[q] + kH, v[q], vec32);
+#pragma unroll
+      for (int q = 0; q < N; q++)
+        if ((pass >> q) & 1u) hit |= (test_words<kH, kW>(v[q], key[q]) ? 1u : 0u) << q;
+    } else if constexpr (!kS.fixed_words && kS.ng >= 2) {
+      constexpr int kG = kS.ng / 2;
+      constexpr int kSlots = kG > kS.ng - kG ? kG : kS.ng - kG;  // words held per key and phase
+      Word x[N][kSlots];
+      auto load_groups = [&](auto lo_c, auto hi_c, int q) {
+        constexpr int Lo = decltype(lo_c)::value, Hi = decltype(hi_c)::value;
+        static_for<kS.ng>([&](auto G) {
+          constexpr int g = decltype(G)::value;
+          if constexpr (g >= Lo && g < Hi) {
+            const Word* p = base[q] + group_word<g>(key[q]);
+            if constexpr (sizeof(Word) == 8) {
+              x[q][g - Lo] = ld_weak_64(p);
+            } else {
+              x[q][g - Lo] = static_cast<Word>(ld_weak_32(p));
+            }
+          }
+        });
+      };
+      auto test_loaded = [&](auto lo_c, auto hi_c, int q) {
+        constexpr int Lo = decltype(lo_c)::value, Hi = decltype(hi_c)::value;
+        bool ok = true;
+        static_for<kS.ng>([&](auto G) {
+          constexpr int g = decltype(G)::value;
+          if constexpr (g >= Lo && g < Hi) {
+            const Word m = group_mask<g>(key[q]);
+            ok &= (x[q][g - Lo] & m) == m;
+          }
+        });
+        return ok;
+      };
+      using C0 = std::integral_constant<int, 0>;
+      using CG = std::integral_constant<int, kG>;
+      using CN = std::integral_constant<int, kS.ng>;
+#pragma unroll
+      for (int q = 0; q < N; q++) load_groups(C0{}, CG{}, q);
+      uint32_t pass = 0;
+#pragma unroll
+      for (int q = 0; q < N; q++) pass |= (test_loaded(C0{}, CG{}, q) ? 1u : 0u) << q;
+#pragma unroll
+      for (int q = 0; q < N; q++)
+        if ((pass >> q) & 1u) load_groups(CG{}, CN{}, q);
+#pragma unroll
+      for (int q = 0; q < N; q++)
+        if ((pass >> q) & 1u) hit |= (test_loaded(CG{}, CN{}, q) ? 1u : 0u) << q;
+    } else {
+#pragma unroll
+      for (int q = 0; q < N; q++) hit |= (test_block<false>(base[q], key[q], vec32) ? 1u : 0u) << q;
+    }
+    return hit;
+  }
+
   // The same test against a copy of the filter in shared memory (plan 4):
   // plain loads, which the compiler issues as shared-memory loads.
   __device__ __forceinline__ static bool contains_shared(const void* sfilter, const ProbeArgs& a, uint32_t key) {
