@@ -267,15 +267,16 @@ __host__ __device__ inline SegChunks seg_chunks(const PartArgs& pa) {
   return s;
 }
 
-// Runs fn(key, position) over every pair of the segments: CTAs take whole
-// chunks from a queue (one atomic per chunk), in range order, so the chunks in
-// flight are the ones next to each other and the filter range they read stays
-// in L2 (a fixed grid-stride assignment lets slow and fast CTAs drift apart
-// over two or more ranges, whose words then evict each other).  The ranges'
-// fill counts are read into shared memory once per CTA; pairs are read two
-// per 16-byte load.  The queue counter (PartHeader::chunk_ctr) must be zero.
-template <class Fn>
-__device__ __forceinline__ void for_each_pair(const SegChunks& s, Fn fn) {
+// Runs chunk(q, cnt) for every non-empty chunk of the segments (q: its pairs
+// as 16-byte vectors of two, cnt: its pairs): CTAs take whole chunks from a
+// queue (one atomic per chunk), in range order, so the chunks in flight are
+// the ones next to each other and the filter range they read stays in L2 (a
+// fixed grid-stride assignment lets slow and fast CTAs drift apart over two
+// or more ranges, whose words then evict each other).  The ranges' fill
+// counts are read into shared memory once per CTA.  The queue counter
+// (PartHeader::chunk_ctr) must be zero.
+template <class Chunk>
+__device__ __forceinline__ void for_each_chunk(const SegChunks& s, Chunk chunk) {
   __shared__ uint32_t s_filled[kMaxRanges];  // pairs in each segment (fill, capped at the capacity)
   __shared__ uint32_t s_chunk;
   for (uint32_t r = threadIdx.x; r < s.n_ranges; r += blockDim.x) {
@@ -298,50 +299,34 @@ __device__ __forceinline__ void for_each_pair(const SegChunks& s, Fn fn) {
     const uint32_t filled = s_filled[r];
     if (filled <= j0) continue;
     const uint32_t cnt = filled - j0 < kPartChunk ? filled - j0 : kPartChunk;
-    const uint4* q = p4 + static_cast<uint64_t>(r) * half_seg + (j0 >> 1);
+    chunk(p4 + static_cast<uint64_t>(r) * half_seg + (j0 >> 1), cnt);
+  }
+}
+
+// fn(key, position) for every pair of the segments, two pairs per 16-byte load.
+template <class Fn>
+__device__ __forceinline__ void for_each_pair(const SegChunks& s, Fn fn) {
+  for_each_chunk(s, [&](const uint4* q, uint32_t cnt) {
     for (uint32_t v = threadIdx.x; 2 * v < cnt; v += blockDim.x) {
       const uint4 x = __ldcs(q + v);
       fn(x.x, x.y);
       if (2 * v + 1 < cnt) fn(x.z, x.w);
     }
-  }
+  });
 }
 
 // for_each_pair for warp-cooperative callbacks: every lane of the CTA calls
-// fn(key, valid) the same number of times (valid = false past the chunk's end),
-// and CTAs of 256 threads take whole chunks from the same queue.
+// fn(key, valid) the same number of times (valid = false past the chunk's end).
 template <class Fn>
 __device__ __forceinline__ void for_each_pair_warp(const SegChunks& s, Fn fn) {
-  __shared__ uint32_t s_filled[kMaxRanges];
-  __shared__ uint32_t s_chunk;
-  for (uint32_t r = threadIdx.x; r < s.n_ranges; r += blockDim.x) {
-    const uint64_t cap = r + 1 < s.n_ranges ? s.seg_cap : s.last_cap;
-    const uint32_t fill = s.hdr->fill[r];
-    s_filled[r] = fill < cap ? fill : static_cast<uint32_t>(cap);
-  }
-  const uint4* p4 = reinterpret_cast<const uint4*>(s.pairs);
-  const uint64_t half_seg = s.seg_cap >> 1;
-  unsigned int* ctr = const_cast<unsigned int*>(&s.hdr->chunk_ctr);
-  for (;;) {
-    if (threadIdx.x == 0) s_chunk = atomicAdd(ctr, 1u);
-    __syncthreads();
-    const uint32_t c = s_chunk;
-    __syncthreads();
-    if (c >= s.n_chunks) break;
-    uint32_t r = c / s.chunks_per_seg;
-    if (r >= s.n_ranges) r = s.n_ranges - 1;
-    const uint32_t j0 = (c - r * s.chunks_per_seg) * kPartChunk;
-    const uint32_t filled = s_filled[r];
-    if (filled <= j0) continue;
-    const uint32_t cnt = filled - j0 < kPartChunk ? filled - j0 : kPartChunk;
-    const uint4* q = p4 + static_cast<uint64_t>(r) * half_seg + (j0 >> 1);
+  for_each_chunk(s, [&](const uint4* q, uint32_t cnt) {
     for (uint32_t vb = 0; 2 * vb < cnt; vb += blockDim.x) {
       const uint32_t v = vb + threadIdx.x;
       const uint4 x = 2 * v < cnt ? __ldcs(q + v) : make_uint4(0, 0, 0, 0);
       fn(x.x, 2 * v < cnt);
       fn(x.z, 2 * v + 1 < cnt);
     }
-  }
+  });
 }
 
 // Runs fn(key, logical position) over the keys of every tile whose run of the
