@@ -464,15 +464,16 @@ dtlg_status launch_probe(const dtlg_filter* f, const uint64_t* words, const uint
 // Build plan of a blocked Bloom or blocked cuckoo filter (one block per key)
 // for n keys: 1 = one kernel of global atomics, 2 = keys grouped by L2-sized
 // block range first (the probe's partition).  Automatic: the partitioned
-// build for Bloom filters beyond 160 MiB and batches of >= 2^20 keys (512 MiB,
-// 2^28 keys: 10.97 -> 6.56 ms; 256 MiB: 4.46 -> 3.31 ms; 64 MiB stays with plan
-// 1, 0.82 against 0.90 ms).  A blocked cuckoo key takes one or two
+// build for Bloom filters beyond 80 MiB and batches of >= 2^20 keys (u64 w=8
+// s=8 k=8, plan 1 -> plan 2: 512 MiB from 2^28 keys 10.55 -> 4.07 ms; 256 MiB
+// 4.23 -> 2.07 ms; 96 MiB (12 bits/key, MAGIC) 1.22 -> 1.09 ms; 64 MiB stays
+// with plan 1, 0.51 against 0.60 ms).  A blocked cuckoo key takes one or two
 // compare-and-swaps, too few to repay the partition (256 MiB, 2^26 keys:
 // 2.60 -> 2.70 ms), so its plan 2 is only taken on request.
 int block_build_plan(const dtlg_filter* f, uint64_t n) {
   if (f->build_mode == 1 || f->build_mode == 2) return f->build_mode;
   const uint64_t bytes = (f->d.m_actual + 7) / 8;
-  return (f->bk != nullptr && n >= kTwoPassMinKeys && bytes > (160ull << 20)) ? 2 : 1;
+  return (f->bk != nullptr && n >= kTwoPassMinKeys && bytes > (80ull << 20)) ? 2 : 1;
 }
 
 int grid_for(uint64_t items, int sms) {

@@ -402,8 +402,13 @@ struct BloomOps {
   // with one bit each, 2^26 keys into 8 MiB build at 82.6 Gkeys/s this way
   // against 23.6 (and into 512 MiB at 24.5 against 6.7).  All 32 lanes call it.
   static constexpr bool kLaneInsert = kS.ng >= 2 && kS.ng <= 32 && (32 % kS.ng) == 0;
-  struct LaneStage {            // per warp, in shared memory
-    Word mask[32 * kS.ng];      // [key lane][group]
+  // Per warp, in shared memory.  Entry (key lane l, group g) sits at
+  // g * 32 + (l ^ (g * 32 / kS.ng)): a lane's stores of one group are 32
+  // consecutive entries, and the loads of a round, kS.ng groups of each of
+  // 32 / kS.ng keys, fall in distinct banks (a [key][group] layout made every
+  // store a 16-way bank conflict for 8 u64 groups).
+  struct LaneStage {
+    Word mask[32 * kS.ng];
     uint8_t word[32 * kS.ng];   // word of the group in its block (hashed layouts)
     uint32_t blk[32];           // block of each lane's key
   };
@@ -411,12 +416,14 @@ struct BloomOps {
                                                       LaneStage& st) {
     static_assert(kLaneInsert, "groups per key must divide the warp");
     constexpr int kNg = kS.ng;
+    constexpr uint32_t kPer = 32 / kNg;  // keys per round
     const uint32_t lane = threadIdx.x & 31u;
     st.blk[lane] = block_index(key * mul_const(0), a);
     static_for<kNg>([&](auto G) {
       constexpr int g = decltype(G)::value;
-      st.mask[lane * kNg + g] = valid ? group_mask<g>(key) : Word(0);
-      if constexpr (!kS.fixed_words) st.word[lane * kNg + g] = static_cast<uint8_t>(group_word<g>(key));
+      const uint32_t e = g * 32 + (lane ^ (g * kPer));
+      st.mask[e] = valid ? group_mask<g>(key) : Word(0);
+      if constexpr (!kS.fixed_words) st.word[e] = static_cast<uint8_t>(group_word<g>(key));
     });
     // with fixed words, this lane's group (lane % kNg) always has the same word
     uint32_t wl = 0;
@@ -427,12 +434,14 @@ struct BloomOps {
       });
     }
     __syncwarp();
+    const uint32_t g = lane % kNg;  // this lane's group in every round
 #pragma unroll
     for (int j = 0; j < kNg; j++) {
-      const uint32_t i = j * 32 + lane;  // group i % kNg of the key of lane i / kNg
-      const Word m = st.mask[i];
-      const uint32_t w = kS.fixed_words ? wl : st.word[i];
-      if (m) atomic_or_word<Word>(static_cast<Word*>(filter) + static_cast<uint64_t>(st.blk[i / kNg]) * kW + w, m);
+      const uint32_t kl = j * kPer + lane / kNg;  // lane of the key
+      const uint32_t e = g * 32 + (kl ^ (g * kPer));
+      const Word m = st.mask[e];
+      const uint32_t w = kS.fixed_words ? wl : st.word[e];
+      if (m) atomic_or_word<Word>(static_cast<Word*>(filter) + static_cast<uint64_t>(st.blk[kl]) * kW + w, m);
     }
     __syncwarp();
   }

@@ -191,7 +191,7 @@ dtlg_status dtlg_batch_contains_gather(const dtlg_filter* f, const uint64_t* fil
 dtlg_status dtlg_set_probe_options(dtlg_filter* f, int mode, int variant);
 /* Build plan of a blocked Bloom or blocked cuckoo filter (no counterpart in
  * the reference, whose batch_insert is one loop): 0 = automatic (2 for Bloom
- * filters beyond 160 MiB and batches of >= 2^20 keys, else 1), 1 = one kernel of
+ * filters beyond 80 MiB and batches of >= 2^20 keys, else 1), 1 = one kernel of
  * global atomics, 2 = keys first grouped by ~8 MiB block range (the
  * partitioned probe's partition, ~8.3 bytes per key of workspace from the
  * library's stream-ordered pool; without room there, plan 1), then inserted

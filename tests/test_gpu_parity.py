@@ -255,7 +255,7 @@ def test_large_filter_property():
 
 
 def test_partitioned_build_large_filter():
-    """Filters beyond 160 MiB are built through the partition automatically:
+    """Filters beyond 80 MiB are built through the partition automatically:
     the same words as the one-kernel build (and, on a sample, the oracle's
     probe of them), for a sectorized and a zoned layout, POW2 and MAGIC."""
     for (wb, w, s_, z, k), m in (((8, 8, 8, 1, 8), 1 << 31), ((8, 8, 8, 2, 8), (3 << 29) + 4096)):
