@@ -76,7 +76,7 @@ constexpr uint32_t kItemBuild = 0;   // y: the filter's build tile
 constexpr uint32_t kItemRange = 1;   // y: the range of a staged filter
 constexpr uint32_t kItemProbe = 2;   // y: the global probe tile
 constexpr uint32_t kItemCompact = 3; // y: the global compact tile (look-back word)
-// Probe keys a thread tests together (BloomOps::testn_weak): their first
+// Probe keys a thread tests together (BloomOps::testn): their first
 // loads are all in flight before any is tested.  512-filter mix, probe phase:
 // 7.15 ms one at a time, 6.62 ms by two; four spill at the 64-register bound.
 constexpr int kTestN = 2;
@@ -411,7 +411,7 @@ __global__ void __launch_bounds__(kBatchThreads, 4) batched_kernel(const __grid_
             uint32_t hit = 0;
 #pragma unroll
             for (int g0 = 0; g0 < 4; g0 += kTestN)
-              hit |= BloomOps<Cfg>::template testn_weak<kTestN>(base + g0, k + g0, vec32) << g0;
+              hit |= BloomOps<Cfg>::template testn<kTestN, false>(base + g0, k + g0, (1u << kTestN) - 1u, vec32) << g0;
 #pragma unroll
             for (int q = 0; q < 4; q++) fl |= ((((hit >> q) & 1u) && k0 + i0 + q < d.n_probe) ? 1u : 0u) << q;
           }

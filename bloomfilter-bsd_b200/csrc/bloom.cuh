@@ -277,25 +277,40 @@ struct BloomOps {
     return ok;
   }
 
-  // test_block<false> for N keys at once: the N first halves (or first
-  // groups) are loaded before any of them is tested, then the second halves of
-  // the keys that passed, so a thread has N gathers in flight instead of one
-  // (the batched kernel runs at half the SM's warp slots).  Bit q of the
-  // result: key q matches.
-  template <int N>
-  __device__ __forceinline__ static uint32_t testn_weak(const Word* const* base, const uint32_t* key, bool vec32) {
+  // test_block<NC> for N keys at once: the N first halves (or first groups)
+  // are loaded before any of them is tested, then the second halves of the
+  // keys that passed, so a thread has N gathers in flight instead of one (for
+  // kernels that run at half the SM's warp slots).  Only the keys whose bit is
+  // set in `live` are loaded and tested.  Bit q of the result: key q matches.
+  // (In the 64-register bitmask kernel, at the same half occupancy, four keys
+  // per thread this way made L2-resident probes slower: 8 MiB u64 w=8 s=8 k=8,
+  // 182 -> 151 Gkeys/s.)
+  template <int N, bool NC>
+  __device__ __forceinline__ static uint32_t testn(const Word* const* base, const uint32_t* key, uint32_t live,
+                                                   bool vec32, bool l1na = false) {
     uint32_t hit = 0;
+    auto one_by_one = [&]() {
+#pragma unroll
+      for (int q = 0; q < N; q++)
+        if ((live >> q) & 1u) hit |= (test_block<NC>(base[q], key[q], vec32, l1na) ? 1u : 0u) << q;
+    };
     if constexpr (kHalves) {
+      if (NC && !vec32) {  // the read-only path tests halves only with 256-bit loads
+        one_by_one();
+        return hit;
+      }
       constexpr int kH = kW / 2;
       Word v[N][kH];
 #pragma unroll
-      for (int q = 0; q < N; q++) load_block<Word, kH, false>(base[q], v[q], vec32);
+      for (int q = 0; q < N; q++)
+        if ((live >> q) & 1u) load_block<Word, kH, NC>(base[q], v[q], vec32, l1na);
       uint32_t pass = 0;
 #pragma unroll
-      for (int q = 0; q < N; q++) pass |= (test_words<0, kH>(v[q], key[q]) ? 1u : 0u) << q;
+      for (int q = 0; q < N; q++)
+        if ((live >> q) & 1u) pass |= (test_words<0, kH>(v[q], key[q]) ? 1u : 0u) << q;
 #pragma unroll
       for (int q = 0; q < N; q++)
-        if ((pass >> q) & 1u) load_block<Word, kH, false>(base[q] + kH, v[q], vec32);
+        if ((pass >> q) & 1u) load_block<Word, kH, NC>(base[q] + kH, v[q], vec32, l1na);
 #pragma unroll
       for (int q = 0; q < N; q++)
         if ((pass >> q) & 1u) hit |= (test_words<kH, kW>(v[q], key[q]) ? 1u : 0u) << q;
@@ -310,9 +325,9 @@ struct BloomOps {
           if constexpr (g >= Lo && g < Hi) {
             const Word* p = base[q] + group_word<g>(key[q]);
             if constexpr (sizeof(Word) == 8) {
-              x[q][g - Lo] = ld_weak_64(p);
+              x[q][g - Lo] = NC ? __ldg(reinterpret_cast<const unsigned long long*>(p)) : ld_weak_64(p);
             } else {
-              x[q][g - Lo] = static_cast<Word>(ld_weak_32(p));
+              x[q][g - Lo] = static_cast<Word>(NC ? __ldg(reinterpret_cast<const unsigned int*>(p)) : ld_weak_32(p));
             }
           }
         });
@@ -333,10 +348,12 @@ struct BloomOps {
       using CG = std::integral_constant<int, kG>;
       using CN = std::integral_constant<int, kS.ng>;
 #pragma unroll
-      for (int q = 0; q < N; q++) load_groups(C0{}, CG{}, q);
+      for (int q = 0; q < N; q++)
+        if ((live >> q) & 1u) load_groups(C0{}, CG{}, q);
       uint32_t pass = 0;
 #pragma unroll
-      for (int q = 0; q < N; q++) pass |= (test_loaded(C0{}, CG{}, q) ? 1u : 0u) << q;
+      for (int q = 0; q < N; q++)
+        if ((live >> q) & 1u) pass |= (test_loaded(C0{}, CG{}, q) ? 1u : 0u) << q;
 #pragma unroll
       for (int q = 0; q < N; q++)
         if ((pass >> q) & 1u) load_groups(CG{}, CN{}, q);
@@ -344,8 +361,7 @@ struct BloomOps {
       for (int q = 0; q < N; q++)
         if ((pass >> q) & 1u) hit |= (test_loaded(CG{}, CN{}, q) ? 1u : 0u) << q;
     } else {
-#pragma unroll
-      for (int q = 0; q < N; q++) hit |= (test_block<false>(base[q], key[q], vec32) ? 1u : 0u) << q;
+      one_by_one();
     }
     return hit;
   }
