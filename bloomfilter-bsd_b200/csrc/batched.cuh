@@ -41,6 +41,7 @@
 #pragma once
 
 #include <cstdint>
+#include <type_traits>
 
 #include "bloom.cuh"
 #include "probe.cuh"
@@ -102,6 +103,17 @@ __device__ __forceinline__ void dispatch_cfg(uint32_t id, F&& f) {
     f(Cfg0{});
   } else if constexpr (sizeof...(Rest) > 0) {
     dispatch_cfg<Rest...>(id - 1, f);
+  }
+}
+
+// f(std::bool_constant<MAGIC>) for the filter's addressing mode: the block
+// index is then computed without a run-time branch on it.
+template <class F>
+__device__ __forceinline__ void dispatch_addr(const Addr& a, F&& f) {
+  if (a.magic_mode) {
+    f(std::true_type{});
+  } else {
+    f(std::false_type{});
   }
 }
 
@@ -170,7 +182,7 @@ __device__ __forceinline__ uint32_t block_exclusive_scan(uint32_t* v, uint32_t n
 // keys goes to its bucket as consecutive (coalesced) stores; one atomic per
 // (tile, range) reserves the run's place in the bucket.
 //   smem: s_cnt / s_gbase [kBatchMaxRanges] + s_keys [kBatchTile] = 32 KiB.
-template <class Cfg>
+template <class Cfg, bool MAGIC>
 __device__ __forceinline__ void scatter_tile(const BatchDesc& d, uint64_t k0, unsigned char* smem,
                                              uint32_t* s_warp) {
   constexpr int kRounds = kBatchTile / (kBatchThreads * 4);
@@ -192,7 +204,7 @@ __device__ __forceinline__ void scatter_tile(const BatchDesc& d, uint64_t k0, un
       key[r * 4 + q] = k[q];
       slot[r * 4 + q] = 0xffffffffu;
       if (k0 + i0 + q < d.n_build) {
-        const uint32_t rg = block_index(k[q] * mul_const(0), d.addr) >> d.range_shift;
+        const uint32_t rg = block_index_of<MAGIC>(k[q] * mul_const(0), d.addr) >> d.range_shift;
         slot[r * 4 + q] = (rg << 12) | atomicAdd(&s_cnt[rg], 1u);
       }
     }
@@ -210,7 +222,7 @@ __device__ __forceinline__ void scatter_tile(const BatchDesc& d, uint64_t k0, un
   __syncthreads();
   for (uint32_t sl = threadIdx.x; sl < n_valid; sl += kBatchThreads) {
     const uint32_t kk = s_keys[sl];
-    const uint32_t rg = block_index(kk * mul_const(0), d.addr) >> d.range_shift;
+    const uint32_t rg = block_index_of<MAGIC>(kk * mul_const(0), d.addr) >> d.range_shift;
     const uint32_t pos = s_gbase[rg] + (sl - s_cnt[rg]);
     if (pos < d.bucket_cap) {
       d.bucket[static_cast<uint64_t>(rg) * d.bucket_cap + pos] = kk;
@@ -221,7 +233,7 @@ __device__ __forceinline__ void scatter_tile(const BatchDesc& d, uint64_t k0, un
 }
 
 // Builds range rg of a staged filter in shared memory and ORs it into the words.
-template <class Cfg>
+template <class Cfg, bool MAGIC>
 __device__ __forceinline__ void build_range(const BatchDesc& d, uint32_t rg, unsigned char* smem) {
   using Word = typename Cfg::word_t;
   constexpr uint32_t kW = Cfg::kW;
@@ -252,7 +264,7 @@ __device__ __forceinline__ void build_range(const BatchDesc& d, uint32_t rg, uns
     for (int u = 0; u < kU; u++) {
       if (i0 + u * kBatchThreads + threadIdx.x >= cnt) break;
       const uint32_t key = kk[u];
-      const uint32_t lb = block_index(key * mul_const(0), d.addr) - blk0;
+      const uint32_t lb = block_index_of<MAGIC>(key * mul_const(0), d.addr) - blk0;
       const uint32_t swz = (lb >> 1) & (kW - 1);
       Word* base = s_w + static_cast<uint64_t>(lb) * kW;
       static_for<BloomOps<Cfg>::kS.ng>([&](auto G) {
@@ -332,7 +344,7 @@ __global__ void __launch_bounds__(kBatchThreads, 4) batched_kernel(const __grid_
       dispatch_cfg<Cfgs...>(d.cfg, [&](auto c) {
         using Cfg = decltype(c);
         if (d.staged) {
-          scatter_tile<Cfg>(d, k0, s_dyn, s_wtot);
+          dispatch_addr(d.addr, [&](auto m) { scatter_tile<Cfg, decltype(m)::value>(d, k0, s_dyn, s_wtot); });
           return;
         }
         using Ops = BloomOps<Cfg>;
@@ -371,7 +383,9 @@ __global__ void __launch_bounds__(kBatchThreads, 4) batched_kernel(const __grid_
 
     if (kind == kItemRange) {
       wait_counter(&a.built[f], d.n_build_tiles, &a.ctl[2]);
-      dispatch_cfg<Cfgs...>(d.cfg, [&](auto c) { build_range<decltype(c)>(d, it.y, s_dyn); });
+      dispatch_cfg<Cfgs...>(d.cfg, [&](auto c) {
+        dispatch_addr(d.addr, [&](auto m) { build_range<decltype(c), decltype(m)::value>(d, it.y, s_dyn); });
+      });
       __syncthreads();
       if (threadIdx.x == 0) {
         __threadfence();
@@ -392,8 +406,9 @@ __global__ void __launch_bounds__(kBatchThreads, 4) batched_kernel(const __grid_
       const uint32_t n_words = (d.n_probe + 31u) / 32u;
       // blocks of >= 32 bytes are read with 256-bit loads when the words are 32-byte aligned
       const bool vec32 = (reinterpret_cast<uintptr_t>(d.words) & 31u) == 0;
-      dispatch_cfg<Cfgs...>(d.cfg, [&](auto c) {
+      dispatch_cfg<Cfgs...>(d.cfg, [&](auto c) { dispatch_addr(d.addr, [&](auto m) {
         using Cfg = decltype(c);
+        constexpr bool MAGIC = decltype(m)::value;
         const uint4* k4 = reinterpret_cast<const uint4*>(d.probe_keys + k0);
 #pragma unroll 1
         for (int r = 0; r < kRounds; r++) {
@@ -405,7 +420,7 @@ __global__ void __launch_bounds__(kBatchThreads, 4) batched_kernel(const __grid_
             const typename Cfg::word_t* base[4];
 #pragma unroll
             for (int q = 0; q < 4; q++) {
-              const uint32_t blk = block_index(k[q] * mul_const(0), d.addr);
+              const uint32_t blk = block_index_of<MAGIC>(k[q] * mul_const(0), d.addr);
               base[q] = static_cast<const typename Cfg::word_t*>(d.words) + static_cast<uint64_t>(blk) * Cfg::kW;
             }
             uint32_t hit = 0;
@@ -423,7 +438,7 @@ __global__ void __launch_bounds__(kBatchThreads, 4) batched_kernel(const __grid_
           const uint32_t w = local * (kBatchTile / 32) + r * (kBatchThreads * 4 / 32) + warp * 4 + (lane >> 3);
           if ((lane & 7u) == 0 && w < n_words) __stcg(d.mask + w, x);
         }
-      });
+      }); });
       __syncthreads();
       if (threadIdx.x == 0) {
         __threadfence();

@@ -190,6 +190,18 @@ __device__ __forceinline__ uint32_t block_index(uint32_t h, const Addr& a) {
   // mulhi(h, 1) == 0 defines it as block 0.
   return __umulhi(h, a.pow2_mul);
 }
+
+// block_index with the addressing mode fixed at compile time (no run-time
+// branch on it; kernels bound by instruction issue instantiate both).
+template <bool MAGIC>
+__device__ __forceinline__ uint32_t block_index_of(uint32_t h, const Addr& a) {
+  if constexpr (MAGIC) {
+    const uint32_t q = __umulhi(h, a.magic) >> a.shift;
+    return h - q * a.divisor;
+  } else {
+    return __umulhi(h, a.pow2_mul);
+  }
+}
 #endif
 
 }  // namespace dtlg

@@ -103,15 +103,7 @@ __device__ __forceinline__ uint32_t key_range(uint32_t key, const PartArgs& a) {
 // branches on it at run time).
 template <bool MAGIC>
 __device__ __forceinline__ uint32_t key_range_of(uint32_t key, const PartArgs& a) {
-  const uint32_t h = key * a.block_mul;
-  uint32_t b;
-  if (MAGIC) {
-    const uint32_t q = __umulhi(h, a.addr.magic) >> a.addr.shift;
-    b = h - q * a.addr.divisor;
-  } else {
-    b = __umulhi(h, a.addr.pow2_mul);
-  }
-  return b >> a.range_log2;
+  return block_index_of<MAGIC>(key * a.block_mul, a.addr) >> a.range_log2;
 }
 
 // Shared memory of one scatter CTA.
