@@ -270,6 +270,14 @@ __device__ __forceinline__ void build_range(const BatchDesc& d, uint32_t rg, uns
       static_for<BloomOps<Cfg>::kS.ng>([&](auto G) {
         constexpr int g = decltype(G)::value;
         Word* p = base + (BloomOps<Cfg>::template group_word<g>(key) ^ swz);
+        constexpr Group grp = BloomOps<Cfg>::kS.g[g];
+        if constexpr (sizeof(Word) == 8 && grp.nbit == 1) {
+          // one bit: one 32-bit atomic on the half that holds it, no test
+          constexpr BitDraw b = grp.bit[0];
+          const uint32_t bit = ((hash_sel<b.sel>(key) >> b.shift) & ((1u << b.bits) - 1u)) + b.off;
+          atomicOr(reinterpret_cast<uint32_t*>(p) + (bit >> 5), 1u << (bit & 31u));
+          return;
+        }
         const Word m = BloomOps<Cfg>::template group_mask<g>(key);
         if constexpr (sizeof(Word) == 8) {
           // 32-bit shared-memory atomics on the halves that have bits to set
