@@ -418,7 +418,7 @@ __global__ void __launch_bounds__(kBatchThreads, 4) batched_kernel(const __grid_
         using Cfg = decltype(c);
         constexpr bool MAGIC = decltype(m)::value;
         const uint4* k4 = reinterpret_cast<const uint4*>(d.probe_keys + k0);
-#pragma unroll 1
+#pragma unroll 2
         for (int r = 0; r < kRounds; r++) {
           const uint32_t i0 = r * (kBatchThreads * 4) + threadIdx.x * 4u;
           uint32_t fl = 0;
