@@ -118,10 +118,17 @@ def test_cuckoo_2p26(ref, t, lf):
     rf = ref.cuckoo(t, b, m)
     assert rf is not None and f.block_cnt() % 2 == 1 and f.is_magic()
     bk = keygen.build_keys_torch(n, SEED)
-    # the reference's build (single thread: its inserts are not thread-safe)
-    table = np.zeros(f.alloc_words(), dtype=np.uint64)
-    assert (rf.word_cnt * 4 + 12) <= table.nbytes
-    assert rf.insert(table, host(bk)), "the reference's build lost keys"
+    # the reference's build (single thread: its inserts are not thread-safe).
+    # Its kicks draw from a random generator it seeds itself, so at load 0.95
+    # an attempt now and then ends with a key it cannot place; another attempt
+    # (the generator moves on) is a new random build of the same keys.
+    for attempt in range(3):
+        table = np.zeros(f.alloc_words(), dtype=np.uint64)
+        assert (rf.word_cnt * 4 + 12) <= table.nbytes
+        if rf.insert(table, host(bk)):
+            break
+    else:
+        raise AssertionError("the reference's build lost keys in 3 attempts")
     assert rf.count_occupied(table) == n
     # the GPU's probe of the reference-built table == the reference's probe
     words = torch.from_numpy(table.view(np.int64)).cuda()
