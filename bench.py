@@ -86,18 +86,27 @@ def parse():
     ap.add_argument("--log2-build", type=int, default=None, help="Bloom workloads: log2 of the build keys")
     ap.add_argument("--bits-per-key", type=int, default=None, help="Bloom workloads: filter bits per build key")
     ap.add_argument("--hit-ratio", type=float, default=None, help="Bloom workloads: fraction of member probes")
+    ap.add_argument("--layout", default=None,
+                    help="Bloom workloads: the filter layout as WORD_BYTES,W,S,Z,K (e.g. 4,16,8,1,8 = u32 words, "
+                         "16 per block, 8 sectors, 1 zone, k=8)")
     args = ap.parse_args()
-    overrides = (args.log2_build, args.bits_per_key, args.hit_ratio)
+    overrides = (args.log2_build, args.bits_per_key, args.hit_ratio, args.layout)
     if any(v is not None for v in overrides):
         # a variant of a Bloom workload (the shapes of the sectorized config:
         # n in {2^22, 2^26, 2^28}, 8/12/16 bits per key, 1/10/50 % hits)
         if args.workload not in WORKLOADS:
-            ap.error("--log2-build / --bits-per-key / --hit-ratio apply to Bloom workloads only")
+            ap.error("--log2-build / --bits-per-key / --hit-ratio / --layout apply to Bloom workloads only")
         wb, w, s_, z, k, ln, bpk, lp, hit = WORKLOADS[args.workload]
         ln = ln if args.log2_build is None else args.log2_build
         bpk = bpk if args.bits_per_key is None else args.bits_per_key
         hit = hit if args.hit_ratio is None else args.hit_ratio
         name = f"{args.workload}_n{ln}_b{bpk}_h{round(hit * 100)}"
+        if args.layout is not None:
+            try:
+                wb, w, s_, z, k = (int(v) for v in args.layout.split(","))
+            except ValueError:
+                ap.error("--layout takes WORD_BYTES,W,S,Z,K")
+            name += f"_u{wb * 8}w{w}s{s_}z{z}k{k}"
         WORKLOADS[name] = (wb, w, s_, z, k, ln, bpk, lp, hit)
         args.workload = name
     return args

@@ -150,6 +150,32 @@ __device__ __forceinline__ void load_block(const Word* base, Word (&v)[W], bool 
   }
 }
 
+// Groups of schedule `s` whose word lies in 32-byte chunk c of the block
+// (chunk_words words per chunk).
+constexpr int chunk_groups(const Schedule& s, int chunk_words, int c) {
+  int n = 0;
+  for (uint32_t g = 0; g < s.ng; g++)
+    if (static_cast<int>(s.g[g].wconst) / chunk_words == c) n++;
+  return n;
+}
+
+// True for hashed-word layouts (zoned, s < w) of 64-byte blocks in which
+// every group picks its word from two neighbours within one 32-byte chunk,
+// the groups in chunk order, and some chunk holds two or more groups (see
+// BloomOps::kChunked).
+constexpr bool chunked_layout(const Schedule& s, int w, int word_bytes) {
+  const int bytes = w * word_bytes, cw = 32 / word_bytes;
+  if (s.fixed_words || bytes != 64) return false;
+  int prev = 0, most = 0;
+  for (uint32_t g = 0; g < s.ng; g++) {
+    const int lo = s.g[g].wconst, hi = lo + (1 << s.g[g].wbits) - 1;
+    if (s.g[g].wbits > 1 || lo / cw != hi / cw || lo / cw < prev) return false;
+    prev = lo / cw;
+  }
+  for (int c = 0; c < bytes / 32; c++) most = chunk_groups(s, cw, c) > most ? chunk_groups(s, cw, c) : most;
+  return most >= 2;  // with one group per chunk the per-group loads are as few
+}
+
 template <class Cfg>
 struct BloomOps {
   using Word = typename Cfg::word_t;
@@ -235,9 +261,73 @@ struct BloomOps {
   // for them.
   static constexpr bool kHalves = kS.fixed_words && kW * static_cast<int>(sizeof(Word)) >= 64;
 
+  // Layouts whose words the hash picks (zoned, s < w) in 64-byte blocks,
+  // where each group picks one of two neighbouring words of a 32-byte chunk
+  // known at compile time (zones and sectors of 16 bytes: u64 w=8 z=4 or
+  // s=4, u32 w=16 z=8 or s=8): the chunk is read with one 256-bit load and
+  // each group's word is picked from it in registers, instead of one load per
+  // group.  Random loads cost the L1 about one wavefront per cache line and
+  // instruction, whatever their width, so these layouts need half the load
+  // instructions or fewer.  The groups of chunk 0 come first (zones and
+  // sectors are drawn in block order); they are tested before chunk 1 is
+  // loaded.  Measured on B200 (2^28 probes, 10 % hits, 8 MiB / 256 MiB,
+  // Gkeys/s, per-group loads -> chunks): u64 w=8 z=4 k=8 162.8 -> 170.9 /
+  // 91.4 -> 108.1; u64 w=8 s=4 k=8 91.4 -> 152.4 / 76.2 -> 74.3; u32 w=16 s=8
+  // k=8 101.8 -> 203.7 / 80.3 -> 88.8.  Wider picks (four or eight words:
+  // u64 s=2, u32 s=2, u32 z=4), 32-byte blocks and more than 8 bits per key
+  // hold more registers, spill in the 32-register kernels and were slower or
+  // no faster (u64 w=8 s=2 k=8 at 256 MiB 78.6 -> 47.1), so they keep the
+  // per-group loads.
+  static constexpr int kChunkWords = 32 / static_cast<int>(sizeof(Word));
+  static constexpr bool kChunked = chunked_layout(kS, kW, static_cast<int>(sizeof(Word))) && Cfg::kK <= 8;
+  static constexpr int kChunk0 = chunk_groups(kS, kChunkWords, 0);  // groups tested against chunk 0
+
+  // Group G's word, picked from the words c[] of its chunk.
+  template <int G>
+  __device__ __forceinline__ static Word chunk_word(const Word (&c)[kChunkWords], uint32_t key) {
+    constexpr Group g = kS.g[G];
+    constexpr int lo = g.wconst % kChunkWords;
+    Word x = c[lo];
+    if constexpr (g.wbits > 0) {
+      const uint32_t j = (hash_sel<g.wsel>(key) >> g.wshift) & ((1u << g.wbits) - 1u);
+      static_for<(1 << g.wbits) - 1>([&](auto J) {
+        constexpr int jj = decltype(J)::value + 1;
+        if (j == jj) x = c[lo + jj];
+      });
+    }
+    return x;
+  }
+
+  // Groups [Lo, Hi) against the words of their chunk.
+  template <int Lo, int Hi>
+  __device__ __forceinline__ static bool test_chunk(const Word (&c)[kChunkWords], uint32_t key) {
+    bool ok = true;
+    static_for<kS.ng>([&](auto G) {
+      constexpr int g = decltype(G)::value;
+      if constexpr (g >= Lo && g < Hi) {
+        const Word m = group_mask<g>(key);
+        ok &= (chunk_word<g>(c, key) & m) == m;
+      }
+    });
+    return ok;
+  }
+
   // The key's bits in the block at `base`; NC selects the read-only load path.
   template <bool NC>
   __device__ __forceinline__ static bool test_block(const Word* base, uint32_t key, bool vec32, bool l1na = false) {
+    if constexpr (kChunked) {
+      if (vec32) {
+        Word c[kChunkWords];
+        load_block<Word, kChunkWords, NC>(base, c, true, l1na);
+        if (!test_chunk<0, kChunk0>(c, key)) return false;
+        if constexpr (kChunk0 < static_cast<int>(kS.ng)) {
+          load_block<Word, kChunkWords, NC>(base + kChunkWords, c, true, l1na);
+          return test_chunk<kChunk0, kS.ng>(c, key);
+        } else {
+          return true;
+        }
+      }
+    }
     if constexpr (kHalves) {
       constexpr int kH = kW / 2;
       if constexpr (NC) {
@@ -294,6 +384,29 @@ struct BloomOps {
       for (int q = 0; q < N; q++)
         if ((live >> q) & 1u) hit |= (test_block<NC>(base[q], key[q], vec32, l1na) ? 1u : 0u) << q;
     };
+    if constexpr (kChunked) {
+      if (vec32) {
+        Word c[N][kChunkWords];
+#pragma unroll
+        for (int q = 0; q < N; q++)
+          if ((live >> q) & 1u) load_block<Word, kChunkWords, NC>(base[q], c[q], true, l1na);
+        uint32_t pass = 0;
+#pragma unroll
+        for (int q = 0; q < N; q++)
+          if ((live >> q) & 1u) pass |= (test_chunk<0, kChunk0>(c[q], key[q]) ? 1u : 0u) << q;
+        if constexpr (kChunk0 == static_cast<int>(kS.ng)) {
+          return pass;
+        } else {
+#pragma unroll
+          for (int q = 0; q < N; q++)
+            if ((pass >> q) & 1u) load_block<Word, kChunkWords, NC>(base[q] + kChunkWords, c[q], true, l1na);
+#pragma unroll
+          for (int q = 0; q < N; q++)
+            if ((pass >> q) & 1u) hit |= (test_chunk<kChunk0, kS.ng>(c[q], key[q]) ? 1u : 0u) << q;
+          return hit;
+        }
+      }
+    }
     if constexpr (kHalves) {
       if (NC && !vec32) {  // the read-only path tests halves only with 256-bit loads
         one_by_one();

@@ -124,6 +124,35 @@ def test_shared_memory_plan():
                     assert np.array_equal(gpu_probe(f, words, pk, 77, pad), exp), (wb, w, s_, z, k, kib, mode, pad)
 
 
+@pytest.mark.parametrize("layout", [(8, 8, 8, 4, 8), (8, 8, 4, 1, 8), (4, 16, 8, 1, 8), (8, 8, 8, 1, 8),
+                                    (8, 8, 2, 1, 8), (4, 16, 16, 2, 8)])
+def test_probe_filter_base_16_not_32_byte_aligned(layout):
+    """Filter words that start 16 bytes past a 32-byte boundary: the probes
+    read 32-byte chunks and half blocks with 256-bit loads only from 32-byte
+    aligned words and fall back to narrower loads otherwise.  Both forms give
+    the oracle's list in every plan (the chunked layouts u64 w=8 z=4 and s=4,
+    u32 w=16 s=8 included)."""
+    wb, w, s_, z, k = layout
+    m = 12 * 40000
+    ob = O.Bloom(wb, w, s_, z, k, m)
+    f = F.construct(F.blocked_bloomfilter_config(k=k, word_size=wb, word_cnt_per_block=w, sector_cnt=s_,
+                                                 zone_cnt=z), m)
+    bk = keygen.build_keys(40000, 8)
+    rw = ob.alloc()
+    ob.insert(rw, bk)
+    buf = torch.zeros(len(rw) + 4, dtype=torch.int64, device="cuda")
+    assert buf.data_ptr() % 32 == 0
+    for shift in (0, 2):  # words at a 32-byte boundary, then 16 bytes past one
+        words = buf[shift:shift + len(rw)]
+        words.copy_(dev_words(rw))
+        pk, _ = keygen.probe_keys(40000, 70001, 0.3, 8)
+        exp = ob.batch_contains(rw, pk, 5)
+        for mode, variant in ((1, -1), (2, 0), (2, 1), (3, 0), (3, 1), (4, -1)):
+            f.set_probe_options(mode, variant)
+            assert np.array_equal(gpu_probe(f, words, pk, 5), exp), (layout, shift, mode, variant)
+        f.set_probe_options(0, -1)
+
+
 @pytest.mark.parametrize("n", [0, 1, 2, 3, 4, 5, 31, 1023, 1024, 4095, 4096, 4097, 8191, 65537, 300001])
 def test_probe_lengths_and_alignment(n):
     ob = O.Bloom(8, 8, 8, 1, 8, 3 * (1 << 16))
