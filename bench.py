@@ -664,10 +664,24 @@ def run_dtlg(args):
             dist.all_reduce(et, op=dist.ReduceOp.MAX)
         e_ms = float(et.item())
         chunks = -(-P // (1 << 24))
+        # the bound of the host-buffer path: one plain copy of the same pinned
+        # keys to the device (median of 3), the PCIe host-to-device rate
+        dst = torch.empty_like(keys)
+        h2d = []
+        for _ in range(3):
+            a.record(stream)
+            dst.copy_(keys_h, non_blocking=True)
+            b.record(stream)
+            torch.cuda.synchronize()
+            h2d.append(P * 4 / (a.elapsed_time(b) / 1e3) / 1e9)
+        del dst
+        h2d_gbs = sorted(h2d)[1]
         result["e2e"] = {"value": round(world * P / (e_ms / 1e3) / 1e9, 3), "unit": "Gkeys/s",
                          "ms_per_step": round(e_ms, 3), "h2d_bytes_per_step": P * 4,
                          "d2h_bytes_per_step": count * 4 + 8 * chunks,
-                         "api": "dtlg_batch_contains_host (pinned host keys -> host positions)"}
+                         "api": "dtlg_batch_contains_host (pinned host keys -> host positions)",
+                         "pcie_h2d_gbs": round(h2d_gbs, 2),
+                         "frac_of_pcie_h2d": round(P * 4 / (e_ms / 1e3) / 1e9 / h2d_gbs, 4)}
         result["gpu_launches"] += e_steps * chunks * L.dtlg_probe_kernel_count(f._h, 1 << 24)
 
     # the reference's CPU path on this host (rank 0, N=1 only): its rate on a
