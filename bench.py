@@ -18,6 +18,7 @@ max-over-ranks of the timings).
 """
 import argparse
 import json
+import math
 import os
 import statistics
 import subprocess
@@ -44,6 +45,12 @@ WORKLOADS = {
 CUCKOO_WORKLOADS = {
     # name: (bits per tag, tags per bucket, log2 n, load factor, log2 probes, hit ratio)
     "cuckoo_dram": (16, 4, 26, 0.95, 28, 0.10),
+    # the same with 12-bit tags (6-byte buckets, some straddle a 32-byte
+    # sector) and 8-bit tags (4-byte buckets); 8-bit tags at load 0.93: with
+    # 255 tag values the alternate buckets of a bucket are too few to place
+    # 2^26 keys at 0.95
+    "cuckoo_dram_t12": (12, 4, 26, 0.95, 28, 0.10),
+    "cuckoo_dram_t8": (8, 4, 26, 0.93, 28, 0.10),
 }
 BCF_WORKLOADS = {
     # name: (block bytes, tag bits, associativity, log2 n, log2 m bits, log2 probes, hit ratio)
@@ -124,6 +131,14 @@ def cuckoo_bits(n, t, b, lf):
         if f.block_cnt() % 2 == 1 and f.is_magic() and f.block_cnt() * b * lf >= n:
             return m
     raise RuntimeError("no odd MAGIC bucket count found")
+
+
+def cuckoo_bucket_sectors(bucket_bytes):
+    """Mean 32-byte sectors one bucket of a packed cuckoo table touches: 1
+    when buckets tile the sectors (4 or 8 bytes), more when some straddle a
+    sector boundary (6-byte buckets: 2 of every 16 do)."""
+    period = 32 // math.gcd(32, bucket_bytes)
+    return sum(1 + ((bucket_bytes * i) % 32 + bucket_bytes > 32) for i in range(period)) / period
 
 
 def bcf_sectors(block_bytes, t, a):
@@ -486,7 +501,8 @@ def run_dtlg(args):
         n_build, P = 1 << ln, 1 << lp
         m = cuckoo_bits(n_build, tag_bits, slots, lf)
         f = dtlg.cf(m, tag_bits, slots)
-        block_bytes, sectors = (tag_bits * slots + 7) // 8, 2   # two buckets, 8-byte aligned: one sector each
+        block_bytes = (tag_bits * slots + 7) // 8
+        sectors = 2 * cuckoo_bucket_sectors(block_bytes)   # two buckets
     elif args.workload in CLASSIC_WORKLOADS:
         ck, ln, bpk, lp, hit, cmagic = CLASSIC_WORKLOADS[args.workload]
         n_build, P = 1 << ln, 1 << lp
