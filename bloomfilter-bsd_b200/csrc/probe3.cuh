@@ -108,8 +108,7 @@ __device__ __forceinline__ uint32_t key_range_of(uint32_t key, const PartArgs& a
 
 // Shared memory of one scatter CTA.
 struct ScatterSmem {
-  uint32_t keys[kPartTile];            // the tile's keys sorted by range
-  uint16_t idx[kPartTile];             // their tile-local indexes
+  unsigned long long kv[kPartTile];    // the tile sorted by range: key | tile-local index << 32
   uint32_t cur[kMaxRanges];            // counts, then the placement cursor
   uint32_t lim[kMaxRanges];            // sorted slots below this go to the segment, the rest overflow
   unsigned long long dst[kMaxRanges];  // pair index of sorted slot 0 for the range's run
@@ -120,8 +119,8 @@ struct ScatterSmem {
 // One pass: per tile, count the keys of every range, reserve the tile's run of
 // each range in its segment (one global atomic per tile and range), sort the
 // tile by range in shared memory and write every run with consecutive
-// addresses.  Shared memory holds the sorted keys and their 12-bit tile
-// positions (24 KiB).  The kernel is bound by instruction issue, so the
+// addresses.  Shared memory holds the sorted keys with their 12-bit tile
+// positions, one 64-bit word each (32 KiB).  The kernel is bound by instruction issue, so the
 // addressing mode is a template parameter (POW2 or MAGIC, chosen by the
 // launch), the tile's index arithmetic is 32-bit, a key's range is computed
 // once for the count and the placement (kept as bytes), and each range's
@@ -200,18 +199,21 @@ __device__ __forceinline__ void scatter_tile(const PartArgs& a, uint32_t tile, S
     for (int q = 0; q < 4; q++) {
       if (li + q >= lo && li + q < hi) {
         const uint32_t slot = atomicAdd(&S.cur[(rr[i] >> (8 * q)) & 0xffu], 1u);
-        S.keys[slot] = k[q];
-        S.idx[slot] = static_cast<uint16_t>(li + q);
+        S.kv[slot] = static_cast<unsigned long long>(li + q) << 32 | k[q];
       }
     }
   }
   __syncthreads();
+  // the placement cursors are not read below: clear them for the next tile
+  // (the barrier after the write-out orders this before its counts)
+  if (threadIdx.x < kMaxRanges) S.cur[threadIdx.x] = 0;
   const uint32_t nv = S.valid;
   const uint32_t pos0 = static_cast<uint32_t>(tile_pos - a.pre);  // logical position of tile index 0 (mod 2^32)
   for (uint32_t sl = threadIdx.x; sl < nv; sl += THREADS) {
-    const uint32_t key = S.keys[sl];
+    const unsigned long long kv = S.kv[sl];
+    const uint32_t key = static_cast<uint32_t>(kv);
     const uint32_t r = key_range_of<MAGIC>(key, a);
-    const uint2 pr = make_uint2(key, pos0 + S.idx[sl]);
+    const uint2 pr = make_uint2(key, pos0 + static_cast<uint32_t>(kv >> 32));
     if (sl < S.lim[r]) {
       __stcs(a.pairs + (S.dst[r] + sl), pr);
     } else {
@@ -225,14 +227,18 @@ __device__ __forceinline__ void scatter_tile(const PartArgs& a, uint32_t tile, S
 template <bool MAGIC, int THREADS = kPartThreads>
 static __global__ void __launch_bounds__(THREADS, 2048 / THREADS) part_scatter_kernel(const __grid_constant__ PartArgs a) {
   __shared__ ScatterSmem S;
+  // The counters start at zero; each tile clears them again for the next one
+  // while it writes its runs out, so a tile needs no barrier of its own for it.
+  if (threadIdx.x < kMaxRanges) S.cur[threadIdx.x] = 0;
+  if (threadIdx.x == 0) S.over = 0;
+  __syncthreads();
   for (uint32_t tile = blockIdx.x; tile < a.n_tiles; tile += gridDim.x) {
-    if (threadIdx.x < kMaxRanges) S.cur[threadIdx.x] = 0;
-    if (threadIdx.x == 0) S.over = 0;
-    __syncthreads();
     scatter_tile<MAGIC, THREADS>(a, tile, S);
     if (threadIdx.x == 0) {
+      // S.over is next written in the next tile's write-out, three barriers on
       a.tile_overflow[tile] = S.over;
       if (S.over) atomicAdd(&a.hdr->overflow_tiles, 1u);
+      S.over = 0;
     }
   }
 }
