@@ -133,6 +133,16 @@ def cuckoo_bits(n, t, b, lf):
     raise RuntimeError("no odd MAGIC bucket count found")
 
 
+def host_chunks(n, chunk=1 << 24):
+    """Key counts of the pieces dtlg_batch_contains_host streams n keys in
+    (csrc/host_pipeline.cu): chunks of 2^24 keys, the last 2^24 keys or fewer
+    in four pieces."""
+    full = (n - 1) // chunk if n > chunk else 0
+    tail = n - full * chunk
+    piece = max(1, -(-tail // 4))
+    return [chunk] * full + [min(piece, tail - i) for i in range(0, tail, piece)]
+
+
 def cuckoo_bucket_sectors(bucket_bytes):
     """Mean 32-byte sectors one bucket of a packed cuckoo table touches: 1
     when buckets tile the sectors (4 or 8 bytes), more when some straddle a
@@ -679,7 +689,7 @@ def run_dtlg(args):
         if world > 1:
             dist.all_reduce(et, op=dist.ReduceOp.MAX)
         e_ms = float(et.item())
-        chunks = -(-P // (1 << 24))
+        chunks = host_chunks(P)
         # the bound of the host-buffer path: one plain copy of the same pinned
         # keys to the device (median of 3), the PCIe host-to-device rate
         dst = torch.empty_like(keys)
@@ -694,11 +704,11 @@ def run_dtlg(args):
         h2d_gbs = sorted(h2d)[1]
         result["e2e"] = {"value": round(world * P / (e_ms / 1e3) / 1e9, 3), "unit": "Gkeys/s",
                          "ms_per_step": round(e_ms, 3), "h2d_bytes_per_step": P * 4,
-                         "d2h_bytes_per_step": count * 4 + 8 * chunks,
+                         "d2h_bytes_per_step": count * 4 + 8 * len(chunks),
                          "api": "dtlg_batch_contains_host (pinned host keys -> host positions)",
                          "pcie_h2d_gbs": round(h2d_gbs, 2),
                          "frac_of_pcie_h2d": round(P * 4 / (e_ms / 1e3) / 1e9 / h2d_gbs, 4)}
-        result["gpu_launches"] += e_steps * chunks * L.dtlg_probe_kernel_count(f._h, 1 << 24)
+        result["gpu_launches"] += e_steps * sum(L.dtlg_probe_kernel_count(f._h, c) for c in chunks)
 
     # the reference's CPU path on this host (rank 0, N=1 only): its rate on a
     # bounded sample, and its whole match list of the same 2^28 keys against

@@ -82,7 +82,14 @@ dtlg_status dtlg_batch_contains_host(const dtlg_filter* f, const uint64_t* words
   Pipeline* p = nullptr;
   if (dtlg_status st = pipe_for_device(&p)) return st;
   std::lock_guard<std::mutex> lk(p->mu);
-  const uint64_t chunks = (n + kChunk - 1) / kChunk;
+  // Chunks of kChunk keys, but the last kChunk keys (or fewer) in four
+  // pieces: what runs after the last host-to-device copy (its probe and the
+  // copy back of its positions) is then a quarter as long.
+  const uint64_t full = n > kChunk ? (n - 1) / kChunk : 0;  // whole chunks before the tail
+  const uint64_t tail_keys = n - full * kChunk;
+  const uint64_t piece = std::max<uint64_t>(1, (tail_keys + 3) / 4);
+  const uint64_t chunks = full + (tail_keys + piece - 1) / piece;
+  auto chunk_start = [&](uint64_t i) { return i < full ? i * kChunk : full * kChunk + (i - full) * piece; };
   uint64_t written = 0;
   dtlg_status result = DTLG_OK;
   auto drain = [&](uint64_t j) -> dtlg_status {  // copy out the positions of chunk j
@@ -98,8 +105,8 @@ dtlg_status dtlg_batch_contains_host(const dtlg_filter* f, const uint64_t* words
   };
   for (uint64_t i = 0; i < chunks && result == DTLG_OK; i++) {
     const int b = static_cast<int>(i % kBufs);
-    const uint64_t start = i * kChunk;
-    const uint32_t len = static_cast<uint32_t>(std::min<uint64_t>(kChunk, n - start));
+    const uint64_t start = chunk_start(i);
+    const uint32_t len = static_cast<uint32_t>(std::min<uint64_t>(i < full ? kChunk : piece, n - start));
     if (i >= kBufs) {  // buffer b was last used by chunk i - kBufs
       PIPE_CUDA(cudaStreamWaitEvent(p->h2d, p->probed[b], 0));
       PIPE_CUDA(cudaStreamWaitEvent(stream, p->out_done[b], 0));

@@ -37,3 +37,13 @@ def test_layout_rejected_outside_bloom_workloads(monkeypatch):
     monkeypatch.setattr(sys, "argv", ["bench.py", "--workload", "sectorized_l2", "--layout", "8,8"])
     with pytest.raises(SystemExit):
         bench.parse()
+
+
+def test_host_chunks_mirror_the_pipeline():
+    # chunks of 2^24 keys, the last 2^24 (or fewer) in four pieces
+    assert bench.host_chunks(1 << 28) == [1 << 24] * 15 + [1 << 22] * 4
+    assert bench.host_chunks(4) == [1, 1, 1, 1]
+    assert bench.host_chunks(5) == [2, 2, 1]
+    assert bench.host_chunks((1 << 24) * 2 + 12345) == [1 << 24] * 2 + [3087, 3087, 3087, 3084]
+    for n in (1, 3, 1 << 24, (1 << 24) + 1, 123456789):
+        assert sum(bench.host_chunks(n)) == n
